@@ -1,0 +1,3 @@
+// Forwarding header of the oracle host AMReX-API shim.
+#pragma once
+#include "amrex_host.H"
