@@ -1,0 +1,161 @@
+/* treesap-b200: C ABI of the B200 single-level explicit integrator.
+ *
+ * Plain C types only (no CUDA, no C++ and no torch types in any signature). Every entry
+ * point returns a ts_status and never throws or aborts; the text of the last failure of a
+ * context is available from ts_context_last_error(). The reference (treesap, header-only
+ * C++20 over AMReX) has no FFI of its own; each entry point below names the reference
+ * interface it stands in for (paths relative to the reference's src/treesap/).
+ *
+ * Threading: one ts_context per host thread. All device work of a context is enqueued on
+ * the context's CUDA stream in call order; *_sync entry points wait for it.
+ *
+ * HBM layout of a field (all state and stage buffers): component-major, [comp][z][y][x] with
+ * x fastest, `ngrow` ghost cells on every face, the x origin shifted by `xoff` (ngrow rounded
+ * up to 16 bytes) so that interior rows start 16-byte aligned, and the row pitch padded to
+ * 16 bytes:  element (i, j, k, c) is at  ((c*pz + k+ngrow)*py + j+ngrow)*px + i+xoff
+ * for i in [-ngrow, n0+ngrow), j in [-ngrow, n1+ngrow), k in [-ngrow, n2+ngrow).
+ */
+#ifndef TREESAP_B200_H
+#define TREESAP_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TS_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define TS_API __attribute__((visibility("default")))
+#else
+#define TS_API
+#endif
+
+typedef enum ts_status {
+    TS_OK = 0,
+    TS_ERR_INVALID_ARGUMENT = 1, /* bad descriptor, size or pointer */
+    TS_ERR_UNSUPPORTED = 2,      /* valid request outside the instantiated model set */
+    TS_ERR_CUDA = 3,             /* a CUDA runtime call failed (text in ts_context_last_error) */
+    TS_ERR_OUT_OF_MEMORY = 4,
+    TS_ERR_DEVICE = 5,           /* a kernel reported an error word (bounded wait expired, bad index) */
+    TS_ERR_NO_DEVICE = 6         /* no usable sm_100 device */
+} ts_status;
+
+typedef enum ts_dtype { TS_F64 = 0, TS_F32 = 1 } ts_dtype;
+typedef enum ts_model { TS_MODEL_WAVE = 0, TS_MODEL_TENSOR_WAVE = 1 } ts_model;
+typedef enum ts_scheme { TS_EULER = 0, TS_RK4 = 1 } ts_scheme;
+typedef enum ts_bc { TS_BC_NOOP = 0, TS_BC_DIRICHLET = 1 } ts_bc;
+typedef enum ts_precision {
+    TS_PRECISION_F64 = 0,      /* plain form: FP64 throughout, the reference's register scheme */
+    TS_PRECISION_F32_STAGE = 1 /* FP32 stage arithmetic and storage, FP64 state and final combination */
+} ts_precision;
+typedef enum ts_init_kind { TS_INIT_STATE = 0, TS_INIT_GAUSSIAN = 1, TS_INIT_FOURIER = 2 } ts_init_kind;
+
+/* ------------------------------------------------------------------ runtime */
+typedef struct ts_context ts_context;
+
+TS_API int ts_abi_version(void);
+TS_API const char* ts_status_string(ts_status s);
+
+/* One device, one stream, one device error word. */
+TS_API ts_status ts_context_create(int device, ts_context** out);
+TS_API ts_status ts_context_destroy(ts_context* ctx);
+/* Waits for all work of the context, then reads and clears the device error word. */
+TS_API ts_status ts_context_sync(ts_context* ctx);
+TS_API const char* ts_context_last_error(const ts_context* ctx);
+/* The context's cudaStream_t and its device error word (int*), for callers that launch
+ * their own kernels (e.g. the header-only C++ front end) on the same stream. */
+TS_API void* ts_context_stream(ts_context* ctx);
+TS_API int* ts_context_error_word(ts_context* ctx);
+TS_API int ts_context_sm_count(const ts_context* ctx);
+
+/* ------------------------------------------------------------------ field layout */
+typedef struct ts_field_layout {
+    int n[3];          /* valid cells per direction */
+    int ngrow;         /* ghost width */
+    int ncomp;
+    int dtype;         /* ts_dtype */
+    int xoff;          /* x index of cell i = 0 within a row, ngrow rounded up to 16 bytes */
+    int reserved;
+    long long px, py, pz; /* padded extents (elements): row pitch, rows per plane, planes per component */
+} ts_field_layout;
+
+/* Fills *out for the given extents (replaces the allocation rule of
+ * SingleLevelIntegrator.hpp:47-49: MultiFab(ba, dm, ncomp, ngrow)). */
+TS_API ts_status ts_field_layout_make(const int n[3], int ngrow, int ncomp, int dtype, ts_field_layout* out);
+TS_API long long ts_field_bytes(const ts_field_layout* layout);
+/* Encodes the TMA descriptor (a 128-byte CUtensorMap) used by the fused stage kernels to
+ * stream a field plane by plane: a 4-d tensor (x, y, z, comp) read in boxes of
+ * (box_x, box_y, 1, ncomp). `base` is a device pointer to the field. */
+TS_API ts_status ts_field_tensor_map(const ts_field_layout* layout, const void* base, int box_x, int box_y,
+                              void* tensor_map_out);
+
+/* ------------------------------------------------------------------ built-in models
+ * The built-in models are ordinary treesap user models (treesap_b200/cpp/rhs/) instantiated
+ * in this library through the header front end:
+ *   TS_MODEL_WAVE         {phi, pi}: phi_t = pi, pi_t = c(x)^2 sum_a D2_aa phi
+ *   TS_MODEL_TENSOR_WAVE  {h_ij, p_ij} (2 x SymRank2Alias): h_t = p,
+ *                         p_t = Lap h - 1/3 delta Lap tr h + 1/2 (d_i d_k h_kj + d_j d_k h_ki)
+ * optionally wrapped in KODecorator{rhs, ko_strength} (order = ngrow) and, when
+ * abl_thickness > 0, built as ABLPDEModel (absorbing layer, Dirichlet(target) ghosts). */
+typedef struct ts_wave_desc {
+    int n[3];
+    double prob_lo[3];
+    double prob_hi[3];
+    int periodic[3];
+    int ngrow;               /* 1..4 */
+    int model;               /* ts_model */
+    double ko_strength;      /* > 0: Kreiss-Oliger dissipation */
+    int abl_thickness;       /* > 0: absorbing layer of this many cells */
+    double abl_max_strength;
+    int abl_profile;         /* 1: s, 2: s^2 */
+    int bc;                  /* ts_bc, for non-periodic faces (forced to Dirichlet(target) by the layer) */
+    double bc_values[12];    /* Dirichlet values / absorbing-layer targets per component */
+    double dt;
+    int scheme;              /* ts_scheme */
+    int precision;           /* ts_precision (TS_PRECISION_F32_STAGE needs TS_RK4) */
+    const double* c2;        /* TS_MODEL_WAVE only: host array of c(x)^2 per valid cell, x fastest; NULL = 1 */
+} ts_wave_desc;
+
+typedef struct ts_integrator ts_integrator;
+
+/* SingleLevelRK4Integrator / SingleLevelEulerIntegrator(model, block_size)
+ * (integrators/SingleLevelRK4Integrator.hpp:65-67, SingleLevelEulerIntegrator.hpp:51-52). */
+TS_API ts_status ts_integrator_create(ts_context* ctx, const ts_wave_desc* desc, ts_integrator** out);
+TS_API ts_status ts_integrator_destroy(ts_integrator* it);
+TS_API int ts_integrator_ncomp(const ts_integrator* it);
+
+/* initialise() (Integrator.hpp:75-78, SingleLevelIntegrator.hpp:75-93): evaluates the
+ * initial condition at cell centres lo + (i + 1/2) dx on the device. init_kind
+ * TS_INIT_GAUSSIAN: nitems pulses {comp, A, w, cx, cy, cz};
+ * TS_INIT_FOURIER: nitems modes {comp, A, kx, ky, kz, phase}. Resets time and step count. */
+TS_API ts_status ts_integrator_initialise(ts_integrator* it, int init_kind, int nitems, const double* items);
+
+/* Valid-cell state, component-major [comp][z][y][x] FP64. `src`/`dst` are host pointers
+ * (pageable or pinned) unless *_is_device is nonzero. set_state resets time and step count. */
+TS_API ts_status ts_integrator_set_state(ts_integrator* it, const double* src, int src_is_device);
+TS_API ts_status ts_integrator_get_state(ts_integrator* it, double* dst, int dst_is_device);
+
+/* step() x nsteps (Integrator.hpp:91-106): ghost fill + computeNewState + swap per step,
+ * enqueued on the context stream (returns without waiting). */
+TS_API ts_status ts_integrator_step(ts_integrator* it, int nsteps);
+
+/* End-to-end call: host state in -> nsteps steps -> host state out, synchronous. */
+TS_API ts_status ts_integrator_run(ts_integrator* it, const double* host_in, int nsteps, double* host_out);
+
+TS_API ts_status ts_integrator_time(const ts_integrator* it, double* time, long long* steps);
+
+/* Device pointer and layout of the current FP64 state (valid after the last enqueued step). */
+TS_API ts_status ts_integrator_state_field(ts_integrator* it, void** device_ptr, ts_field_layout* layout);
+
+/* Capture one step into a CUDA graph and replay it for subsequent ts_integrator_step calls
+ * (enable != 0), or go back to per-kernel launches (enable == 0). */
+TS_API ts_status ts_integrator_use_graph(ts_integrator* it, int enable);
+
+/* Device time of the most recent ts_integrator_step call, measured with CUDA events on the
+ * context stream (valid after ts_context_sync), and the number of kernels it launched. */
+TS_API ts_status ts_integrator_last_step_timing(ts_integrator* it, double* ms, long long* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TREESAP_B200_H */

@@ -1,0 +1,41 @@
+"""Shared fixtures. GPU tests are marked `gpu`; everything else runs on the CPU."""
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a B200 (sm_100a) GPU")
+
+
+@pytest.fixture(scope="session")
+def ctx():
+    from treesap_b200 import Context
+
+    c = Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    """The CPU checker: the reference build when present, else the plain-C restatement."""
+    from oracle import pyoracle
+
+    if not pyoracle.available("port"):
+        pyoracle.build()
+    return pyoracle.Oracle("ref" if pyoracle.available("ref") else "port")
+
+
+@pytest.fixture(scope="session")
+def port_oracle():
+    from oracle import pyoracle
+
+    if not pyoracle.available("port"):
+        pyoracle.build()
+    return pyoracle.Oracle("port")

@@ -1,0 +1,143 @@
+"""Parity of the B200 kernels with the CPU oracle (FP64 plain form: <= 1e-12 relative max-norm).
+
+Every case calls the library through the C ABI (ts_integrator_*) and runs the same seeded
+input through the oracle (the reference's own integrators built on the host, or the
+bit-identical plain-C restatement). Relative max-norm = max|gpu - cpu| / max|cpu|.
+"""
+import itertools
+
+import numpy as np
+import pytest
+
+from treesap_b200 import (TS_BC_DIRICHLET, TS_BC_NOOP, TS_EULER, TS_F32_STAGE, TS_F64, TS_INIT_GAUSSIAN, TS_RK4,
+                          Integrator)
+from treesap_b200.configs import C1_STEPS, c1_desc, c1_pulses, c2_pulses, wave_desc
+
+pytestmark = pytest.mark.gpu
+
+TOL_F64 = 1e-12  # FP64 plain form vs oracle, relative max-norm
+
+
+def relerr(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def smooth_state(shape, seed):
+    """Seeded smooth-ish random state (sum of a few low Fourier modes plus small noise)."""
+    rng = np.random.default_rng(seed)
+    nc, nz, ny, nx = shape
+    z, y, x = np.meshgrid(np.arange(nz) / nz, np.arange(ny) / ny, np.arange(nx) / nx, indexing="ij")
+    s = np.zeros(shape)
+    for c in range(nc):
+        for _ in range(4):
+            k = rng.integers(-2, 3, 3)
+            s[c] += rng.normal() * np.cos(2 * np.pi * (k[0] * x + k[1] * y + k[2] * z) + rng.uniform(0, 6.28))
+        s[c] += 0.01 * rng.standard_normal((nz, ny, nx))
+    return s
+
+
+CASES = list(itertools.product([1, 2, 3, 4], ["periodic", "dirichlet", "abl"], [0.0, 0.15], [TS_RK4, TS_EULER]))
+
+
+@pytest.mark.parametrize("ngrow,bcmode,ko,scheme", CASES)
+def test_fp64_matches_oracle_small(ctx, port_oracle, ngrow, bcmode, ko, scheme):
+    n = (37, 29, 41)  # partial tiles in x, y and uneven z segments
+    kw = dict(prob_lo=(-1.0, 0.0, 0.5), prob_hi=(1.0, 1.0, 2.0), ko=ko, scheme=scheme, dt=0.2 / 41)
+    if bcmode == "periodic":
+        d = wave_desc(n, ngrow, periodic=(1, 1, 1), **kw)
+    elif bcmode == "dirichlet":
+        d = wave_desc(n, ngrow, periodic=(1, 0, 0), bc=TS_BC_DIRICHLET, bc_values=(0.3, -0.2), **kw)
+    else:
+        d = wave_desc(n, ngrow, periodic=(0, 0, 0), abl_thickness=5, abl_max=7.0, abl_profile=2,
+                      bc=TS_BC_DIRICHLET, bc_values=(0.1, 0.0), **kw)
+    state = smooth_state(d.shape(), seed=ngrow * 100 + int(ko * 100) + scheme)
+    it = Integrator(ctx, d)
+    it.set_state(state)
+    it.step(4)
+    gpu = it.get_state()
+    ctx.sync()
+    cpu, _, tcpu = port_oracle.run(d, 4, state=state)
+    assert relerr(gpu, cpu) <= TOL_F64
+    t, s = it.time()
+    assert s == 4 and abs(t - tcpu) == 0.0
+
+
+def test_c1_full_run_matches_oracle(ctx, oracle):
+    """C1: 64^3 periodic, ngrow 2, KO 0.1, RK4, 100 steps from the Gaussian initialiser."""
+    d = c1_desc()
+    it = Integrator(ctx, d)
+    it.initialise(TS_INIT_GAUSSIAN, c1_pulses())
+    it.step(C1_STEPS)
+    gpu = it.get_state()
+    ctx.sync()
+    cpu, _, _ = oracle.run(d, C1_STEPS, items=c1_pulses())
+    assert relerr(gpu, cpu) <= TOL_F64
+
+
+def test_initialise_matches_oracle(ctx, port_oracle):
+    d = wave_desc((33, 20, 27), 3, periodic=(0, 1, 0), bc=TS_BC_DIRICHLET)
+    pul = c2_pulses(7, 5)
+    pul[2, 0] = 1  # one pulse on pi
+    it = Integrator(ctx, d)
+    it.initialise(TS_INIT_GAUSSIAN, pul)
+    gpu = it.get_state()
+    cpu, _, _ = port_oracle.run(d, 0, items=pul)
+    assert relerr(gpu, cpu) <= 1e-14
+
+
+def test_state_roundtrip_is_exact(ctx):
+    d = wave_desc((19, 23, 17), 4, periodic=(0, 0, 1))
+    s = smooth_state(d.shape(), 3)
+    it = Integrator(ctx, d)
+    it.set_state(s)
+    assert np.array_equal(it.get_state(), s)
+
+
+def test_graph_replay_is_bitwise_identical(ctx):
+    d = wave_desc(48, 2, ko=0.1)
+    s = smooth_state(d.shape(), 5)
+    a = Integrator(ctx, d)
+    a.set_state(s)
+    a.step(7)
+    ra = a.get_state()
+    b = Integrator(ctx, d)
+    b.use_graph(True)
+    b.set_state(s)
+    b.step(3)
+    b.step(4)
+    rb = b.get_state()
+    assert np.array_equal(ra, rb)
+    assert b.time()[1] == 7
+
+
+def test_variable_speed_matches_oracle(ctx, port_oracle):
+    d = wave_desc(32, 2, ko=0.1)
+    rng = np.random.default_rng(11)
+    c2 = (1.0 + 0.2 * rng.uniform(-1, 1, (32, 32, 32))) ** 2
+    s = smooth_state(d.shape(), 9)
+    it = Integrator(ctx, d, c2=c2)
+    it.set_state(s)
+    it.step(5)
+    gpu = it.get_state()
+    cpu, _, _ = port_oracle.run(d, 5, state=s, c2=c2)
+    assert relerr(gpu, cpu) <= TOL_F64
+
+
+@pytest.mark.parametrize("bcmode", ["periodic", "abl"])
+def test_fp32_stage_error_vs_fp64(ctx, bcmode):
+    """FP32-stage RK4 vs FP64 GPU path: max-norm relative error <= 1e-6 after 200 steps."""
+    if bcmode == "periodic":
+        mk = lambda p: wave_desc(64, 4, ko=0.2, precision=p)
+    else:
+        mk = lambda p: wave_desc(64, 4, periodic=(0, 0, 0), ko=0.2, abl_thickness=8, abl_max=10.0,
+                                 bc=TS_BC_DIRICHLET, precision=p)
+    pul = c2_pulses(1, 4)
+    out = {}
+    for p in (TS_F64, TS_F32_STAGE):
+        it = Integrator(ctx, mk(p))
+        it.initialise(TS_INIT_GAUSSIAN, pul)
+        it.step(200)
+        out[p] = it.get_state()
+    ctx.sync()
+    e = relerr(out[TS_F32_STAGE], out[TS_F64])
+    assert e <= 1e-6, e

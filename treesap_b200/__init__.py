@@ -1,0 +1,264 @@
+"""ctypes bindings of the treesap-b200 C ABI (include/treesap_b200.h).
+
+The product is the C++20 header front end plus the CUDA library libtreesap_b200.so; this
+module is the thin Python binding that tests and bench.py drive it through. There is no
+CPU fallback: every call goes to the sm_100a kernels of the library, and loading fails
+loudly when the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+__all__ = [
+    "LIB_PATH",
+    "TSError",
+    "WaveDesc",
+    "FieldLayout",
+    "lib",
+    "Context",
+    "Integrator",
+    "TS_EULER",
+    "TS_RK4",
+    "TS_F64",
+    "TS_F32_STAGE",
+    "TS_BC_NOOP",
+    "TS_BC_DIRICHLET",
+    "TS_INIT_GAUSSIAN",
+    "TS_INIT_FOURIER",
+    "TS_MODEL_WAVE",
+    "TS_MODEL_TENSOR_WAVE",
+]
+
+LIB_PATH = Path(__file__).resolve().with_name("libtreesap_b200.so")
+
+TS_OK = 0
+TS_EULER, TS_RK4 = 0, 1
+TS_F64, TS_F32_STAGE = 0, 1
+TS_BC_NOOP, TS_BC_DIRICHLET = 0, 1
+TS_INIT_STATE, TS_INIT_GAUSSIAN, TS_INIT_FOURIER = 0, 1, 2
+TS_MODEL_WAVE, TS_MODEL_TENSOR_WAVE = 0, 1
+STATUS_NAMES = {
+    0: "TS_OK",
+    1: "TS_ERR_INVALID_ARGUMENT",
+    2: "TS_ERR_UNSUPPORTED",
+    3: "TS_ERR_CUDA",
+    4: "TS_ERR_OUT_OF_MEMORY",
+    5: "TS_ERR_DEVICE",
+    6: "TS_ERR_NO_DEVICE",
+}
+
+
+class TSError(RuntimeError):
+    def __init__(self, status: int, what: str, detail: str = ""):
+        self.status = status
+        super().__init__(f"{what}: {STATUS_NAMES.get(status, status)}" + (f" ({detail})" if detail else ""))
+
+
+class WaveDesc(C.Structure):
+    """Mirror of ts_wave_desc."""
+
+    _fields_ = [
+        ("n", C.c_int * 3),
+        ("prob_lo", C.c_double * 3),
+        ("prob_hi", C.c_double * 3),
+        ("periodic", C.c_int * 3),
+        ("ngrow", C.c_int),
+        ("model", C.c_int),
+        ("ko_strength", C.c_double),
+        ("abl_thickness", C.c_int),
+        ("abl_max_strength", C.c_double),
+        ("abl_profile", C.c_int),
+        ("bc", C.c_int),
+        ("bc_values", C.c_double * 12),
+        ("dt", C.c_double),
+        ("scheme", C.c_int),
+        ("precision", C.c_int),
+        ("c2", C.c_void_p),
+    ]
+
+    def ncomp(self) -> int:
+        return 12 if self.model == TS_MODEL_TENSOR_WAVE else 2
+
+    def shape(self) -> tuple[int, int, int, int]:
+        """Valid-state array shape (comp, z, y, x)."""
+        return (self.ncomp(), self.n[2], self.n[1], self.n[0])
+
+
+class FieldLayout(C.Structure):
+    """Mirror of ts_field_layout."""
+
+    _fields_ = [
+        ("n", C.c_int * 3),
+        ("ngrow", C.c_int),
+        ("ncomp", C.c_int),
+        ("dtype", C.c_int),
+        ("xoff", C.c_int),
+        ("reserved", C.c_int),
+        ("px", C.c_longlong),
+        ("py", C.c_longlong),
+        ("pz", C.c_longlong),
+    ]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded C-ABI library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m treesap_b200.build`")
+    L = C.CDLL(str(LIB_PATH))
+    vp, i, d, ll = C.c_void_p, C.c_int, C.c_double, C.c_longlong
+    sig = {
+        "ts_abi_version": (i, []),
+        "ts_status_string": (C.c_char_p, [i]),
+        "ts_context_create": (i, [i, C.POINTER(vp)]),
+        "ts_context_destroy": (i, [vp]),
+        "ts_context_sync": (i, [vp]),
+        "ts_context_last_error": (C.c_char_p, [vp]),
+        "ts_context_stream": (vp, [vp]),
+        "ts_context_error_word": (vp, [vp]),
+        "ts_context_sm_count": (i, [vp]),
+        "ts_field_layout_make": (i, [C.POINTER(i), i, i, i, C.POINTER(FieldLayout)]),
+        "ts_field_bytes": (ll, [C.POINTER(FieldLayout)]),
+        "ts_field_tensor_map": (i, [C.POINTER(FieldLayout), vp, i, i, vp]),
+        "ts_integrator_create": (i, [vp, C.POINTER(WaveDesc), C.POINTER(vp)]),
+        "ts_integrator_destroy": (i, [vp]),
+        "ts_integrator_ncomp": (i, [vp]),
+        "ts_integrator_initialise": (i, [vp, i, i, vp]),
+        "ts_integrator_set_state": (i, [vp, vp, i]),
+        "ts_integrator_get_state": (i, [vp, vp, i]),
+        "ts_integrator_step": (i, [vp, i]),
+        "ts_integrator_run": (i, [vp, vp, i, vp]),
+        "ts_integrator_time": (i, [vp, C.POINTER(d), C.POINTER(ll)]),
+        "ts_integrator_state_field": (i, [vp, C.POINTER(vp), C.POINTER(FieldLayout)]),
+        "ts_integrator_use_graph": (i, [vp, i]),
+        "ts_integrator_last_step_timing": (i, [vp, C.POINTER(d), C.POINTER(ll)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(status: int, what: str, ctx: "Context | None" = None) -> None:
+    if status != TS_OK:
+        detail = ""
+        if ctx is not None and ctx.handle:
+            detail = (lib().ts_context_last_error(ctx.handle) or b"").decode()
+        raise TSError(status, what, detail)
+
+
+class Context:
+    """One device, one CUDA stream (ts_context)."""
+
+    def __init__(self, device: int = 0):
+        self.handle = C.c_void_p()
+        _check(lib().ts_context_create(device, C.byref(self.handle)), "ts_context_create")
+
+    def sync(self) -> None:
+        _check(lib().ts_context_sync(self.handle), "ts_context_sync", self)
+
+    @property
+    def stream(self) -> int:
+        return lib().ts_context_stream(self.handle) or 0
+
+    @property
+    def sm_count(self) -> int:
+        return lib().ts_context_sm_count(self.handle)
+
+    def close(self) -> None:
+        if self.handle:
+            lib().ts_context_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Integrator:
+    """A built-in model integrator (ts_integrator)."""
+
+    def __init__(self, ctx: Context, desc: WaveDesc, c2: np.ndarray | None = None):
+        self.ctx = ctx
+        self.desc = desc
+        self._c2 = None
+        if c2 is not None:
+            self._c2 = np.ascontiguousarray(c2, dtype=np.float64)
+            desc.c2 = self._c2.ctypes.data
+        self.handle = C.c_void_p()
+        _check(lib().ts_integrator_create(ctx.handle, C.byref(desc), C.byref(self.handle)), "ts_integrator_create", ctx)
+        self.shape = desc.shape()
+
+    def initialise(self, kind: int, items: np.ndarray) -> None:
+        items = np.ascontiguousarray(items, dtype=np.float64).reshape(-1, 6)
+        _check(
+            lib().ts_integrator_initialise(self.handle, kind, len(items), items.ctypes.data),
+            "ts_integrator_initialise",
+            self.ctx,
+        )
+
+    def set_state(self, state: np.ndarray) -> None:
+        a = np.ascontiguousarray(state, dtype=np.float64)
+        assert a.shape == self.shape, (a.shape, self.shape)
+        _check(lib().ts_integrator_set_state(self.handle, a.ctypes.data, 0), "ts_integrator_set_state", self.ctx)
+        self.ctx.sync()  # the host buffer may be freed by the caller
+
+    def set_state_device(self, dev_ptr: int) -> None:
+        _check(lib().ts_integrator_set_state(self.handle, dev_ptr, 1), "ts_integrator_set_state", self.ctx)
+
+    def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.shape, dtype=np.float64)
+        _check(lib().ts_integrator_get_state(self.handle, out.ctypes.data, 0), "ts_integrator_get_state", self.ctx)
+        return out
+
+    def step(self, nsteps: int = 1) -> None:
+        _check(lib().ts_integrator_step(self.handle, nsteps), "ts_integrator_step", self.ctx)
+
+    def run(self, host_in: np.ndarray, nsteps: int, host_out: np.ndarray) -> None:
+        _check(
+            lib().ts_integrator_run(self.handle, host_in.ctypes.data, nsteps, host_out.ctypes.data),
+            "ts_integrator_run",
+            self.ctx,
+        )
+
+    def use_graph(self, enable: bool = True) -> None:
+        _check(lib().ts_integrator_use_graph(self.handle, int(enable)), "ts_integrator_use_graph", self.ctx)
+
+    def time(self) -> tuple[float, int]:
+        t, s = C.c_double(), C.c_longlong()
+        _check(lib().ts_integrator_time(self.handle, C.byref(t), C.byref(s)), "ts_integrator_time", self.ctx)
+        return t.value, s.value
+
+    def last_step_timing(self) -> tuple[float, int]:
+        ms, n = C.c_double(), C.c_longlong()
+        _check(lib().ts_integrator_last_step_timing(self.handle, C.byref(ms), C.byref(n)), "timing", self.ctx)
+        return ms.value, n.value
+
+    def state_field(self) -> tuple[int, FieldLayout]:
+        p, L = C.c_void_p(), FieldLayout()
+        _check(lib().ts_integrator_state_field(self.handle, C.byref(p), C.byref(L)), "state_field", self.ctx)
+        return p.value or 0, L
+
+    def close(self) -> None:
+        if self.handle:
+            lib().ts_integrator_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,93 @@
+"""Workload descriptors of the benchmark configurations (seeded synthetic inputs).
+
+  C1  64^3 unit cube, periodic, scalar wave, 4th-order stencils (ngrow 2), KO 0.1, RK4,
+      dt = 0.25 dx, 100 steps; phi0 = exp(-|x - c|^2 / 0.1^2), c = (1/2, 1/2, 1/2), pi0 = 0.
+  C2  256^3 unit cube, scalar wave, 8th-order (ngrow 4), KO 0.2, absorbing layer 16 cells,
+      profile s^2, max strength 10/L, targets 0 (Dirichlet-0 ghosts), RK4 dt = 0.25 dx,
+      1000 steps; phi0 = sum of 8 Gaussians, A ~ U[0.5, 1], w ~ U[0.05, 0.15],
+      c ~ U[0.25, 0.75]^3, pi0 = 0; FP64 and FP32-stage.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import TS_BC_DIRICHLET, TS_BC_NOOP, TS_F64, TS_MODEL_WAVE, TS_RK4, WaveDesc
+
+
+def wave_desc(
+    n,
+    ngrow: int,
+    *,
+    periodic=(1, 1, 1),
+    ko: float = 0.0,
+    abl_thickness: int = 0,
+    abl_max: float = 0.0,
+    abl_profile: int = 2,
+    bc: int = TS_BC_NOOP,
+    bc_values=(0.0, 0.0),
+    dt: float | None = None,
+    cfl: float = 0.25,
+    scheme: int = TS_RK4,
+    precision: int = TS_F64,
+    prob_lo=(0.0, 0.0, 0.0),
+    prob_hi=(1.0, 1.0, 1.0),
+    model: int = TS_MODEL_WAVE,
+) -> WaveDesc:
+    d = WaveDesc()
+    n = (n, n, n) if np.isscalar(n) else tuple(n)
+    d.n[:] = list(n)
+    d.prob_lo[:] = list(prob_lo)
+    d.prob_hi[:] = list(prob_hi)
+    d.periodic[:] = [int(p) for p in periodic]
+    d.ngrow = ngrow
+    d.model = model
+    d.ko_strength = ko
+    d.abl_thickness = abl_thickness
+    d.abl_max_strength = abl_max
+    d.abl_profile = abl_profile
+    d.bc = bc
+    for q, v in enumerate(bc_values):
+        d.bc_values[q] = v
+    dx = (prob_hi[0] - prob_lo[0]) / n[0]
+    d.dt = dt if dt is not None else cfl * dx
+    d.scheme = scheme
+    d.precision = precision
+    d.c2 = None
+    return d
+
+
+def c1_desc(precision: int = TS_F64) -> WaveDesc:
+    return wave_desc(64, 2, ko=0.1, precision=precision)
+
+
+def c1_pulses() -> np.ndarray:
+    return np.array([[0, 1.0, 0.1, 0.5, 0.5, 0.5]], dtype=np.float64)
+
+
+def c2_desc(precision: int = TS_F64, n: int = 256) -> WaveDesc:
+    return wave_desc(
+        n,
+        4,
+        periodic=(0, 0, 0),
+        ko=0.2,
+        abl_thickness=16 if n >= 64 else max(1, n // 8),
+        abl_max=10.0,
+        abl_profile=2,
+        bc=TS_BC_DIRICHLET,
+        bc_values=(0.0, 0.0),
+        precision=precision,
+    )
+
+
+def c2_pulses(seed: int = 2024, npulses: int = 8) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    p = np.zeros((npulses, 6))
+    p[:, 0] = 0
+    p[:, 1] = rng.uniform(0.5, 1.0, npulses)
+    p[:, 2] = rng.uniform(0.05, 0.15, npulses)
+    p[:, 3:6] = rng.uniform(0.25, 0.75, (npulses, 3))
+    return p
+
+
+C1_STEPS = 100
+C2_STEPS = 1000

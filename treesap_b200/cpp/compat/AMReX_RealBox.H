@@ -1,0 +1,3 @@
+// treesap-b200 amrex compatibility layer: forwarding header.
+#pragma once
+#include "AMReX.H"

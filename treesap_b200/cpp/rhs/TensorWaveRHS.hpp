@@ -22,6 +22,8 @@ namespace tsb {
 template <int ngrow_> struct TensorWaveRHS {
     static constexpr int ncomp = 12;
     static constexpr int ngrow = ngrow_;
+    /// Linear in the state and independent of time (eligible for the FP32-stage RK4 form).
+    static constexpr bool is_affine_autonomous = true;
 
     struct Workspace {};
 

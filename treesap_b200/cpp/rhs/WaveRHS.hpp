@@ -42,6 +42,8 @@ template <typename S> struct FieldSpeed {
 template <int ngrow_, typename Speed = UnitSpeed> struct WaveRHS {
     static constexpr int ncomp = 2;
     static constexpr int ngrow = ngrow_;
+    /// Linear in the state and independent of time (eligible for the FP32-stage RK4 form).
+    static constexpr bool is_affine_autonomous = true;
 
     struct Workspace {};
 

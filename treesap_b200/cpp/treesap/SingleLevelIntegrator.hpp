@@ -1,0 +1,207 @@
+// treesap-b200: single-level integrator base (reference SingleLevelIntegrator.hpp:18-188).
+//
+// Owns the FP64 state (state_old / state_new, ncomp components, ngrow ghost cells) in HBM,
+// evaluates the initial condition on the device, fills ghost cells before every step and
+// swaps the state after it. Differences from the reference that do not change results:
+//   * the domain is one box in HBM; block_size is accepted and validated but the work is
+//     decomposed by the stage kernels' tiles instead (the ghost cells that AMReX would
+//     exchange between boxes are interior cells here and hold the same values);
+//   * all device work runs asynchronously on the context's CUDA stream.
+#pragma once
+
+#include <AMReX.H>
+#include <cuda_runtime.h>
+
+#include <optional>
+#include <stdexcept>
+#include <vector>
+
+#include "Integrator.hpp"
+#include "engine/context.hpp"
+#include "engine/field.hpp"
+#include "engine/grid_kernels.cuh"
+#include "engine/stage_kernel.cuh"
+#include "pde-model/PDEModelConcepts.hpp"
+
+namespace treesap {
+
+namespace detail {
+/// Tile shape of the fused stage kernel for a given value type, ghost width and component
+/// count: 32-wide rows (one warp), the tallest tile whose ring of shared-memory planes
+/// leaves room for two CTAs per SM, falling back to one CTA per SM for many components.
+template <typename T, int G, int NC> struct DefaultTile {
+    template <int TY, int P> using C = treesap_b200::TileCfg<32, TY, G, NC, T, P>;
+    static constexpr int kTwoPerSM = 113 * 1024, kOnePerSM = 220 * 1024;
+    using type = std::conditional_t<
+        (C<8, 2>::SMEM <= kTwoPerSM), C<8, 2>,
+        std::conditional_t<(C<4, 2>::SMEM <= kTwoPerSM), C<4, 2>,
+                           std::conditional_t<(C<8, 1>::SMEM <= kOnePerSM), C<8, 1>,
+                                              std::conditional_t<(C<4, 1>::SMEM <= kOnePerSM), C<4, 1>, C<2, 1>>>>>;
+};
+} // namespace detail
+
+template <typename PDEModelType>
+    requires PDEModelConcept<PDEModelType>
+class SingleLevelIntegrator : public Integrator<PDEModelType> {
+  protected:
+    using Base = Integrator<PDEModelType>;
+    using Base::ncomp;
+    using Base::ngrow;
+    using typename Base::BCType;
+    using typename Base::InitType;
+    using typename Base::RHSType;
+    using Base::model;
+    using Base::steps;
+    using Base::time;
+    using Field = treesap_b200::DeviceField<amrex::Real>;
+
+  public:
+    SingleLevelIntegrator(PDEModelType model_, const amrex::IntVect& block_size, ts_context* ctx_ = nullptr)
+        : Base(std::move(model_)), ctx(ctx_ ? ctx_ : treesap_b200::default_context()),
+          geom(model.get_geometry().data()), state_old(extent(), ngrow, ncomp), state_new(extent(), ngrow, ncomp) {
+        for (int d = 0; d < 3; ++d) {
+            if (block_size[d] < 1) throw std::invalid_argument("block_size must be positive");
+            if (geom.domain.length(d) < ngrow) throw std::invalid_argument("domain smaller than the ghost width");
+        }
+        if (geom.domain.smallEnd(0) != 0 || geom.domain.smallEnd(1) != 0 || geom.domain.smallEnd(2) != 0)
+            throw std::invalid_argument("treesap-b200 expects a domain index range starting at 0");
+        const auto& recs = model.get_bc_recs();
+        treesap_b200::cuda_check(cudaMalloc(&bc_recs_dev, sizeof(amrex::BCRec) * (recs.size() ? recs.size() : 1)),
+                                 "cudaMalloc(bc_recs)");
+        if (!recs.empty())
+            treesap_b200::cuda_check(cudaMemcpy(bc_recs_dev, recs.data(), sizeof(amrex::BCRec) * recs.size(),
+                                                cudaMemcpyHostToDevice),
+                                     "cudaMemcpy(bc_recs)");
+    }
+
+    virtual ~SingleLevelIntegrator() {
+        if (staging) cudaFree(staging);
+        if (bc_recs_dev) cudaFree(bc_recs_dev);
+    }
+
+    SingleLevelIntegrator(const SingleLevelIntegrator&) = delete;
+    SingleLevelIntegrator& operator=(const SingleLevelIntegrator&) = delete;
+
+    void configureExporter(const fs::path& path, int export_interval) {
+        exporter.emplace([this](double* host) { get_state(host); }, model.get_geometry(), model.get_comp_names(), path,
+                         export_interval);
+    }
+
+    void initialise_impl() override {
+        const auto& L = state_old.layout();
+        const long long ncell = L.valid_cells();
+        long long blocks = (ncell + 255) / 256;
+        if (blocks > 32LL * sm_count()) blocks = 32LL * sm_count();
+        treesap_b200::init_kernel<ncomp, InitType>
+            <<<int(blocks), 256, 0, stream()>>>(state_old.data(), L, geom, model.get_init());
+        treesap_b200::cuda_check(cudaGetLastError(), "init_kernel launch");
+        steps = 0;
+        time = 0.0;
+    }
+
+    void pre_step() final override {
+        if (exporter) exporter->exportIfNecessary(int(steps), time);
+        FillPatch(state_old, time);
+    }
+
+    amrex::Real step_impl() final override { return computeNewState(model.dt_hint()); }
+
+    void post_step() final override { swap(state_old, state_new); }
+
+    // ---------------------------------------------------------------- treesap-b200 extensions
+    ts_context* context() const { return ctx; }
+    cudaStream_t stream() const { return static_cast<cudaStream_t>(ts_context_stream(ctx)); }
+    int sm_count() const { return ts_context_sm_count(ctx); }
+    const Field& state() const { return state_old; }
+    Field& state() { return state_old; }
+
+    /// Copies the valid cells ([comp][z][y][x], FP64) into state_old; resets time and steps.
+    void set_state(const double* src, bool src_on_device = false) {
+        ensure_staging();
+        const auto& L = state_old.layout();
+        const size_t bytes = sizeof(double) * size_t(L.valid_cells()) * ncomp;
+        treesap_b200::cuda_check(cudaMemcpyAsync(staging, src, bytes,
+                                                 src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                                 stream()),
+                                 "cudaMemcpyAsync(set_state)");
+        treesap_b200::launch_pack(state_old.data(), L, staging, 0, sm_count(), stream());
+        steps = 0;
+        time = 0.0;
+    }
+
+    /// Copies the valid cells of state_old out; waits for the stream when dst is on the host.
+    void get_state(double* dst, bool dst_on_device = false) {
+        ensure_staging();
+        const auto& L = state_old.layout();
+        const size_t bytes = sizeof(double) * size_t(L.valid_cells()) * ncomp;
+        treesap_b200::launch_pack(state_old.data(), L, staging, 1, sm_count(), stream());
+        treesap_b200::cuda_check(cudaMemcpyAsync(dst, staging, bytes,
+                                                 dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                                 stream()),
+                                 "cudaMemcpyAsync(get_state)");
+        if (!dst_on_device) treesap_b200::cuda_check(cudaStreamSynchronize(stream()), "cudaStreamSynchronize");
+    }
+
+    /// Kernel launches enqueued by the last step() (for launch accounting).
+    long long launches_per_step() const { return launches_per_step_; }
+
+    /// Runs the host-side bookkeeping of one step (buffer swaps, clock) without enqueuing any
+    /// device work: used when the step's kernels are replayed from a captured CUDA graph.
+    void step_host_only() {
+        dry_run_ = true;
+        try {
+            this->step();
+        } catch (...) {
+            dry_run_ = false;
+            throw;
+        }
+        dry_run_ = false;
+    }
+
+  protected:
+    virtual amrex::Real computeNewState(amrex::Real dt_hint) = 0;
+
+    /// Ghost fill of an FP64 field with the model's BC functor (SingleLevelIntegrator.hpp:153-163).
+    void FillPatch(Field& f, amrex::Real time_) {
+        ScopedTimer timer("Integrator::FillPatch()");
+        if (dry_run_) return;
+        treesap_b200::launch_ghost_fill(f.data(), f.layout(), geom, model.get_bc(), bc_recs_dev, time_,
+                                        treesap_b200::GhostMode::Functor, sm_count(), stream());
+    }
+
+    const CUtensorMap& tensor_map(const void* base, const treesap_b200::Layout& L, int dtype, int box_x, int box_y) {
+        return tmaps.get(base, L, dtype, box_x, box_y);
+    }
+
+    static const int* extent_of(const amrex::Geometry& g, int* n) {
+        for (int d = 0; d < 3; ++d) n[d] = g.Domain().length(d);
+        return n;
+    }
+    const int* extent() {
+        extent_of(model.get_geometry(), extent_buf);
+        return extent_buf;
+    }
+
+    void ensure_staging() {
+        if (!staging)
+            treesap_b200::cuda_check(
+                cudaMalloc(&staging, sizeof(double) * size_t(state_old.layout().valid_cells()) * ncomp),
+                "cudaMalloc(staging)");
+    }
+
+    ts_context* ctx;
+    int extent_buf[3] = {0, 0, 0};
+    amrex::GeometryData geom;
+    Field state_old;
+    Field state_new;
+    amrex::BCRec* bc_recs_dev = nullptr;
+    double* staging = nullptr;
+    treesap_b200::TensorMapCache tmaps;
+    long long launches_per_step_ = 0;
+    bool dry_run_ = false; // true while step_host_only() runs: no kernel launches
+
+  private:
+    std::optional<PlotExporter> exporter = std::nullopt;
+};
+
+} // namespace treesap

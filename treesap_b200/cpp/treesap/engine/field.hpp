@@ -1,0 +1,113 @@
+// treesap-b200 engine: HBM layout of a field and an owning device buffer.
+//
+// Layout (see include/treesap_b200.h): [comp][z][y][x], x fastest, ngrow ghost cells on every
+// face, x origin shifted by xoff = ngrow rounded up to 16 bytes so interior rows start 16-byte
+// aligned (and TMA boxes that start ngrow cells left of a tile start on a 16-byte boundary),
+// row pitch padded to 16 bytes (TMA stride rule).
+#pragma once
+
+#include <AMReX.H>
+#include <cuda_runtime.h>
+
+#include <stdexcept>
+#include <string>
+
+#include <treesap_b200.h>
+
+namespace treesap_b200 {
+
+struct Layout {
+    int n[3] = {0, 0, 0};
+    int g = 0;
+    int nc = 0;
+    int esize = 8;
+    int xoff = 0;
+    long long px = 0, py = 0, pz = 0;
+
+    AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE long long comp_stride() const { return px * py * pz; }
+    AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE long long index(int i, int j, int k, int c) const {
+        return c * comp_stride() + (long long)(k + g) * px * py + (long long)(j + g) * px + (i + xoff);
+    }
+    AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE long long elements() const { return comp_stride() * nc; }
+    long long bytes() const { return elements() * esize; }
+    long long valid_cells() const { return (long long)n[0] * n[1] * n[2]; }
+
+    static int round_up(int v, int m) { return (v + m - 1) / m * m; }
+    static Layout make(const int n_[3], int g_, int nc_, int esize_) {
+        Layout L;
+        for (int d = 0; d < 3; ++d) L.n[d] = n_[d];
+        L.g = g_;
+        L.nc = nc_;
+        L.esize = esize_;
+        const int a = 16 / esize_;
+        L.xoff = round_up(g_, a);
+        L.px = round_up(L.xoff + n_[0] + g_, a);
+        L.py = n_[1] + 2 * g_;
+        L.pz = n_[2] + 2 * g_;
+        return L;
+    }
+    ts_field_layout to_c(int dtype) const {
+        ts_field_layout c{};
+        for (int d = 0; d < 3; ++d) c.n[d] = n[d];
+        c.ngrow = g;
+        c.ncomp = nc;
+        c.dtype = dtype;
+        c.xoff = xoff;
+        c.px = px;
+        c.py = py;
+        c.pz = pz;
+        return c;
+    }
+};
+
+/// Plain (view-less) Array4 over a field, with AMReX's index convention.
+template <class T> AMREX_GPU_HOST_DEVICE inline amrex::Array4<T> make_array4(T* base, const Layout& L) {
+    return amrex::Array4<T>(base, L.px, L.px * L.py, L.comp_stride(), amrex::Dim3{-L.xoff, -L.g, -L.g},
+                            amrex::Dim3{int(L.px) - L.xoff, L.n[1] + L.g, L.n[2] + L.g}, L.nc);
+}
+
+inline void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+/// Owning, zero-initialised device buffer of one field.
+template <class T> class DeviceField {
+  public:
+    DeviceField() = default;
+    DeviceField(const int n[3], int g, int nc) : L_(Layout::make(n, g, nc, sizeof(T))) {
+        cuda_check(cudaMalloc(&p_, L_.bytes()), "cudaMalloc(field)");
+        cuda_check(cudaMemset(p_, 0, L_.bytes()), "cudaMemset(field)");
+    }
+    DeviceField(DeviceField&& o) noexcept : L_(o.L_), p_(o.p_) { o.p_ = nullptr; }
+    DeviceField& operator=(DeviceField&& o) noexcept {
+        if (this != &o) {
+            release();
+            L_ = o.L_;
+            p_ = o.p_;
+            o.p_ = nullptr;
+        }
+        return *this;
+    }
+    DeviceField(const DeviceField&) = delete;
+    DeviceField& operator=(const DeviceField&) = delete;
+    ~DeviceField() { release(); }
+
+    T* data() const { return p_; }
+    const Layout& layout() const { return L_; }
+    amrex::Array4<T> array() const { return make_array4(p_, L_); }
+    amrex::Array4<const T> const_array() const { return make_array4<const T>(p_, L_); }
+    friend void swap(DeviceField& a, DeviceField& b) noexcept {
+        std::swap(a.L_, b.L_);
+        std::swap(a.p_, b.p_);
+    }
+
+  private:
+    void release() {
+        if (p_) cudaFree(p_);
+        p_ = nullptr;
+    }
+    Layout L_{};
+    T* p_ = nullptr;
+};
+
+} // namespace treesap_b200

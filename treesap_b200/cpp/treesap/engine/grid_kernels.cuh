@@ -1,0 +1,155 @@
+// treesap-b200 engine: ghost fill, initialisation and host-order pack/unpack kernels.
+//
+// Ghost fill (the single-level FillPatch of SingleLevelIntegrator.hpp:153-163): one thread
+// per ghost cell, all components. A ghost cell whose coordinates, wrapped in the periodic
+// directions, land inside the domain takes that valid cell's value; every other ghost cell
+// (outside the domain grown by the ghost width in periodic directions only) is handed to
+// the model's BC functor (DirichletBC.hpp:43-65 writes its values to all components,
+// NoOpBC leaves the cell alone). The ghost cells are enumerated slab by slab so that all
+// z- and y-face writes are contiguous along x:
+//   z slabs: k in [-g,0) u [n2, n2+g), all j, i          (2 g (n1+2g)(n0+2g) cells)
+//   y slabs: k in [0,n2), j in [-g,0) u [n1,n1+g), all i (2 g n2 (n0+2g) cells)
+//   x slabs: k in [0,n2), j in [0,n1), i in [-g,0) u [n0,n0+g)  (2 g n2 n1 cells)
+#pragma once
+
+#include <AMReX.H>
+#include <cuda_runtime.h>
+
+#include "../util/static_for.hpp"
+#include "field.hpp"
+
+namespace treesap_b200 {
+
+enum class GhostMode : int {
+    Functor = 0,     // periodic images + the BC functor outside the domain
+    Homogeneous = 1, // periodic images + zero outside the domain (increments of Dirichlet data)
+    PeriodicOnly = 2 // periodic images only (ghosts outside the domain untouched)
+};
+
+struct GhostCount {
+    long long z, y, x;
+    AMREX_GPU_HOST_DEVICE long long total() const { return z + y + x; }
+};
+
+AMREX_GPU_HOST_DEVICE inline GhostCount ghost_count(const Layout& L) {
+    const long long g = L.g, n0 = L.n[0], n1 = L.n[1], n2 = L.n[2];
+    return {2 * g * (n1 + 2 * g) * (n0 + 2 * g), 2 * g * n2 * (n0 + 2 * g), 2 * g * n2 * n1};
+}
+
+AMREX_GPU_HOST_DEVICE inline void ghost_coords(const Layout& L, long long t, int& i, int& j, int& k) {
+    const GhostCount gc = ghost_count(L);
+    const int g = L.g, n0 = L.n[0], n1 = L.n[1], n2 = L.n[2];
+    if (t < gc.z) {
+        const long long row = n0 + 2 * g, plane = row * (n1 + 2 * g);
+        const int kk = int(t / plane);
+        const long long r = t % plane;
+        j = int(r / row) - g;
+        i = int(r % row) - g;
+        k = kk < g ? kk - g : n2 + (kk - g);
+        return;
+    }
+    t -= gc.z;
+    if (t < gc.y) {
+        const long long row = n0 + 2 * g, plane = row * 2 * g;
+        k = int(t / plane);
+        const long long r = t % plane;
+        const int jj = int(r / row);
+        i = int(r % row) - g;
+        j = jj < g ? jj - g : n1 + (jj - g);
+        return;
+    }
+    t -= gc.y;
+    const long long plane = (long long)n1 * 2 * g;
+    k = int(t / plane);
+    const long long r = t % plane;
+    j = int(r / (2 * g));
+    const int ii = int(r % (2 * g));
+    i = ii < g ? ii - g : n0 + (ii - g);
+}
+
+template <class T, class BC>
+__global__ void ghost_fill_kernel(T* __restrict__ f, const Layout L, const amrex::GeometryData geom, const BC bc,
+                                  const amrex::BCRec* bcr, double time, int mode) {
+    const long long total = ghost_count(L).total();
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        ghost_coords(L, t, i, j, k);
+        int s[3] = {i, j, k};
+        bool inside = true;
+        for (int d = 0; d < 3; ++d) {
+            if (geom.is_periodic[d]) s[d] = ((s[d] % L.n[d]) + L.n[d]) % L.n[d];
+            if (s[d] < 0 || s[d] >= L.n[d]) inside = false;
+        }
+        const long long cs = L.comp_stride();
+        if (inside) {
+            const long long dst = L.index(i, j, k, 0), src = L.index(s[0], s[1], s[2], 0);
+            for (int c = 0; c < L.nc; ++c) f[dst + c * cs] = f[src + c * cs];
+        } else if (mode == int(GhostMode::Homogeneous)) {
+            const long long dst = L.index(i, j, k, 0);
+            for (int c = 0; c < L.nc; ++c) f[dst + c * cs] = T(0);
+        } else if (mode == int(GhostMode::Functor)) {
+            if constexpr (std::is_same_v<T, amrex::Real>) {
+                const amrex::Array4<amrex::Real> dest = make_array4(f, L);
+                bc(amrex::IntVect{i, j, k}, dest, 0, L.nc, geom, time, bcr, 0, 0);
+            }
+        }
+    }
+}
+
+template <class T, class BC>
+void launch_ghost_fill(T* f, const Layout& L, const amrex::GeometryData& geom, const BC& bc, const amrex::BCRec* bcr,
+                       double time, GhostMode mode, int sm_count, cudaStream_t stream) {
+    const long long total = ghost_count(L).total();
+    if (total == 0) return;
+    const int threads = 256;
+    long long blocks = (total + threads - 1) / threads;
+    const long long cap = (long long)sm_count * 16;
+    if (blocks > cap) blocks = cap;
+    ghost_fill_kernel<T, BC><<<int(blocks), threads, 0, stream>>>(f, L, geom, bc, bcr, time, int(mode));
+    cuda_check(cudaGetLastError(), "ghost_fill_kernel launch");
+}
+
+/// initialise(): state(i,j,k,c) = init<c>(lo + (i + 1/2) dx, ...) (SingleLevelIntegrator.hpp:84-92).
+template <int NC, class Init>
+__global__ void init_kernel(double* __restrict__ f, const Layout L, const amrex::GeometryData geom, const Init init) {
+    const long long ncell = (long long)L.n[0] * L.n[1] * L.n[2];
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ncell;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = int(t % L.n[0]), j = int((t / L.n[0]) % L.n[1]), k = int(t / ((long long)L.n[0] * L.n[1]));
+        const double x = geom.prob_lo[0] + (i + 0.5) * geom.dx[0];
+        const double y = geom.prob_lo[1] + (j + 0.5) * geom.dx[1];
+        const double z = geom.prob_lo[2] + (k + 0.5) * geom.dx[2];
+        const long long o = L.index(i, j, k, 0), cs = L.comp_stride();
+        treesap::static_for<NC>([&]<int c>() { f[o + c * cs] = init.template operator()<c>(x, y, z); });
+    }
+}
+
+/// Contiguous valid-cell order [comp][z][y][x] <-> field layout. dir = 0: packed -> field; 1: field -> packed.
+template <class T>
+__global__ void pack_kernel(T* __restrict__ f, const Layout L, T* __restrict__ packed, int dir) {
+    const long long ncell = (long long)L.n[0] * L.n[1] * L.n[2];
+    const long long total = ncell * L.nc;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = int(t / ncell);
+        const long long r = t % ncell;
+        const int i = int(r % L.n[0]), j = int((r / L.n[0]) % L.n[1]), k = int(r / ((long long)L.n[0] * L.n[1]));
+        const long long o = L.index(i, j, k, c);
+        if (dir == 0)
+            f[o] = packed[t];
+        else
+            packed[t] = f[o];
+    }
+}
+
+template <class T>
+void launch_pack(T* f, const Layout& L, T* packed, int dir, int sm_count, cudaStream_t stream) {
+    const long long total = L.valid_cells() * L.nc;
+    long long blocks = (total + 255) / 256;
+    if (blocks > (long long)sm_count * 32) blocks = (long long)sm_count * 32;
+    pack_kernel<T><<<int(blocks), 256, 0, stream>>>(f, L, packed, dir);
+    cuda_check(cudaGetLastError(), "pack_kernel launch");
+}
+
+} // namespace treesap_b200

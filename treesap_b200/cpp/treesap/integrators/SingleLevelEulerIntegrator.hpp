@@ -1,0 +1,47 @@
+// treesap-b200: forward Euler (reference integrators/SingleLevelEulerIntegrator.hpp:28-88):
+// state_new = state_old + dt F(state_old, t), one fused kernel per step.
+#pragma once
+
+#include "../SingleLevelIntegrator.hpp"
+
+namespace treesap {
+
+template <typename PDEModelType>
+    requires PDEModelConcept<PDEModelType>
+class SingleLevelEulerIntegrator : public SingleLevelIntegrator<PDEModelType> {
+    using Base = SingleLevelIntegrator<PDEModelType>;
+    using Base::geom;
+    using Base::model;
+    using Base::ncomp;
+    using Base::ngrow;
+    using Base::state_new;
+    using Base::state_old;
+    using Base::time;
+    using typename Base::RHSType;
+
+  public:
+    using Tile = typename detail::DefaultTile<double, ngrow, ncomp>::type;
+
+    SingleLevelEulerIntegrator(PDEModelType model_, const amrex::IntVect& block_size, ts_context* ctx_ = nullptr)
+        : Base(std::move(model_), block_size, ctx_) {}
+
+  protected:
+    amrex::Real computeNewState(amrex::Real delta_time) override {
+        const auto& L = state_old.layout();
+        treesap_b200::StageParams<double> sp{};
+        sp.in = state_old.data();
+        sp.L = L;
+        sp.geom = geom;
+        sp.time = time;
+        sp.err = ts_context_error_word(this->ctx);
+        treesap_b200::EpiEuler::Params ep{state_new.data(), L, delta_time};
+        const CUtensorMap& tm = this->tensor_map(state_old.data(), L, TS_F64, Tile::BX, Tile::BY);
+        if (!this->dry_run_)
+            treesap_b200::StageLauncher<Tile, RHSType, treesap_b200::EpiEuler>::launch(tm, sp, model.get_rhs(), ep,
+                                                                                   this->sm_count(), this->stream());
+        this->launches_per_step_ = 2;
+        return delta_time;
+    }
+};
+
+} // namespace treesap

@@ -1,0 +1,81 @@
+// treesap-b200: classical RK4 (reference integrators/SingleLevelRK4Integrator.hpp:37-166).
+//
+// Same registers and arithmetic as the reference: init (= state_old), acc (= state_new),
+// arg, arg_next; a = {0, 1/2, 1/2, 1} dt, b = {1/6, 1/3, 1/3, 1/6} dt computed on the host;
+// stage s: k = F(input, t + a_s dt) with input = init (s = 0) or arg (s > 0, after
+// swap(arg_next, arg) and a ghost fill at t + a_s dt); acc = init + b k (s = 0) or
+// acc += b k; arg_next = init + a_{s+1} k (s < 3). Each stage is ONE fused kernel
+// (engine/stage_kernel.cuh); each ghost fill one kernel (engine/grid_kernels.cuh).
+#pragma once
+
+#include "../SingleLevelIntegrator.hpp"
+
+namespace treesap {
+
+template <typename PDEModelType>
+    requires PDEModelConcept<PDEModelType>
+class SingleLevelRK4Integrator : public SingleLevelIntegrator<PDEModelType> {
+    using Base = SingleLevelIntegrator<PDEModelType>;
+    using Base::FillPatch;
+    using Base::geom;
+    using Base::model;
+    using Base::ncomp;
+    using Base::ngrow;
+    using Base::state_new;
+    using Base::state_old;
+    using Base::steps;
+    using Base::time;
+    using typename Base::Field;
+    using typename Base::RHSType;
+
+  public:
+    using Tile = typename detail::DefaultTile<double, ngrow, ncomp>::type;
+
+    SingleLevelRK4Integrator(PDEModelType model_, const amrex::IntVect& block_size, ts_context* ctx_ = nullptr)
+        : Base(std::move(model_), block_size, ctx_), arg(this->extent(), ngrow, ncomp),
+          arg_next(this->extent(), ngrow, ncomp) {}
+
+  private:
+    static constexpr int stage_count = 4;
+    static constexpr double a_fraction[stage_count] = {0.0, 0.5, 0.5, 1.0};
+    static constexpr double b_fraction[stage_count] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+
+  public:
+    amrex::Real computeNewState(amrex::Real delta_time) override {
+        run_stage<0>(delta_time);
+        run_stage<1>(delta_time);
+        run_stage<2>(delta_time);
+        run_stage<3>(delta_time);
+        this->launches_per_step_ = 4 + 4; // 4 stages + 4 ghost fills (one in pre_step)
+        return delta_time;
+    }
+
+  private:
+    template <int s> void run_stage(amrex::Real dt) {
+        const double a_next = dt * a_fraction[(s + 1) % stage_count];
+        const double time_arg = time + dt * a_fraction[s];
+        const double b = dt * b_fraction[s];
+        if constexpr (s > 0) {
+            swap(arg_next, arg);
+            FillPatch(arg, time_arg);
+        }
+        const Field& input = (s == 0) ? state_old : arg;
+        const auto& L = input.layout();
+        treesap_b200::StageParams<double> sp{};
+        sp.in = input.data();
+        sp.L = L;
+        sp.geom = geom;
+        sp.time = time_arg;
+        sp.err = ts_context_error_word(this->ctx);
+        typename treesap_b200::EpiRK4<s>::Params ep{state_new.data(), arg_next.data(), state_old.data(), L, b, a_next};
+        const CUtensorMap& tm = this->tensor_map(input.data(), L, TS_F64, Tile::BX, Tile::BY);
+        if (this->dry_run_) return;
+        treesap_b200::StageLauncher<Tile, RHSType, treesap_b200::EpiRK4<s>>::launch(
+            tm, sp, model.get_rhs(), ep, this->sm_count(), this->stream());
+    }
+
+    Field arg;
+    Field arg_next;
+};
+
+} // namespace treesap

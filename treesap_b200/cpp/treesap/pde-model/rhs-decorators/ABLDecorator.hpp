@@ -1,0 +1,86 @@
+// treesap-b200: absorbing-boundary-layer decorator (reference pde-model/rhs-decorators/ABLDecorator.hpp:24-137).
+//   F -> F - sigma(idx) (arr(idx, comp) - target[comp]),
+//   sigma = 0 inside bulk = domain.grow(-thickness), otherwise
+//   sigma = max_strength * profile(clamp(|idx - clamp(idx, bulk)|_2 / thickness, 0, 1))   (index space).
+#pragma once
+
+#include <cmath>
+
+#include "../../util/stencil.hpp"
+#include "../PDEModelConcepts.hpp"
+#include "NoOpRHS.hpp"
+
+namespace treesap {
+
+/// Trivially copyable profile with profile(0) = 0 and profile(1) = 1, checked at compile time.
+template <typename F>
+concept ABLProfileConcept = std::is_trivially_copyable_v<F> && std::is_default_constructible_v<F> &&
+                            requires(F f, amrex::Real s) {
+                                { f(s) } -> std::convertible_to<amrex::Real>;
+                            } && requires {
+                                requires std::bool_constant<(F{}(0.0) == 0.0)>::value;
+                                requires std::bool_constant<(F{}(1.0) == 1.0)>::value;
+                            };
+
+template <typename RHSType, typename ABLProfileType>
+    requires RHSConcept<RHSType> && ABLProfileConcept<ABLProfileType>
+struct ABLDecorator {
+    static constexpr int ncomp = RHSType::ncomp;
+    static constexpr int ngrow = RHSType::ngrow;
+    static constexpr bool is_affine_autonomous = is_affine_autonomous_v<RHSType>;
+    using Workspace = typename RHSType::Workspace;
+
+    struct ABLData {
+        ABLData(amrex::GpuArray<amrex::Real, ncomp> target_values_, int thickness_, amrex::Real max_strength_,
+                ABLProfileType profile_)
+            : profile(profile_), thickness(thickness_), inv_thickness(1.0 / static_cast<amrex::Real>(thickness_)),
+              max_strength(max_strength_), target_values(target_values_) {}
+
+        ABLProfileType profile;
+        int thickness;
+        amrex::Real inv_thickness;
+        amrex::Real max_strength;
+        amrex::GpuArray<amrex::Real, ncomp> target_values;
+    };
+
+    ABLDecorator(RHSType rhs_, const amrex::Geometry& geom, ABLData data_)
+        : rhs(std::move(rhs_)), data(std::move(data_)), bulk(amrex::grow(geom.Domain(), -data.thickness)) {}
+
+    template <int comp, typename T = amrex::Real>
+    AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE T operator()(const amrex::IntVect idx, amrex::Real time,
+                                                          const amrex::Array4<const T>& arr,
+                                                          const amrex::GeometryData& geom, Workspace& ws) const {
+        return T(rhs.template operator()<comp>(idx, time, arr, geom, ws)) -
+               T(sigma(idx)) * (arr(idx, comp) - T(data.target_values[comp]));
+    }
+
+    AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE amrex::Real sigma(const amrex::IntVect& idx) const {
+        if (bulk.contains(idx)) return 0.0;
+        int d2 = 0;
+        for (int d = 0; d < 3; ++d) {
+            const int v = idx[d] - amrex::Clamp(idx[d], bulk.smallEnd(d), bulk.bigEnd(d));
+            d2 += v * v;
+        }
+        const amrex::Real dist = std::sqrt(static_cast<amrex::Real>(d2));
+        const amrex::Real s = amrex::Clamp(data.inv_thickness * dist, 0.0, 1.0);
+        return data.max_strength * data.profile(s);
+    }
+
+    /// Linear part: the same damping towards zero (targets removed) around the inner linear part.
+    ABLDecorator linear_part() const
+        requires is_affine_autonomous
+    {
+        ABLDecorator l = *this;
+        l.rhs = linear_part_of(rhs);
+        for (int c = 0; c < ncomp; ++c) l.data.target_values[c] = 0.0;
+        return l;
+    }
+
+    RHSType rhs;
+    ABLData data;
+    amrex::Box bulk;
+};
+
+static_assert(RHSConcept<ABLDecorator<NoOpRHS<1, 1>, decltype([](amrex::Real x) constexpr { return x; })>>);
+
+} // namespace treesap

@@ -1,0 +1,49 @@
+// treesap-b200: Kreiss-Oliger dissipation decorator (reference pde-model/rhs-decorators/KODecorator.hpp:32-74).
+//   F -> F + strength * (D_KO^x + D_KO^y + D_KO^z) arr(., comp),   order defaults to ngrow.
+// Aggregate {rhs, strength} like the reference. The operator is templated on the value type
+// of the array so the same decorator runs in the FP32 stage form.
+#pragma once
+
+#include "../../util/stencil.hpp"
+#include "../PDEModelConcepts.hpp"
+#include "NoOpRHS.hpp"
+
+namespace treesap {
+
+template <typename RHSType, int order_ = RHSType::ngrow>
+    requires RHSConcept<RHSType>
+struct KODecorator {
+    static constexpr int ncomp = RHSType::ncomp;
+    static constexpr int ngrow = RHSType::ngrow;
+    static constexpr int order = order_;
+    static_assert(order > 0 && order <= ngrow, "KO order must be in [1, ngrow]");
+    static constexpr bool is_affine_autonomous = is_affine_autonomous_v<RHSType>;
+
+    using Workspace = typename RHSType::Workspace;
+
+    template <int comp, typename T = amrex::Real>
+    AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE T operator()(const amrex::IntVect idx, amrex::Real time,
+                                                          const amrex::Array4<const T>& arr,
+                                                          const amrex::GeometryData& geom, Workspace& ws) const {
+        using namespace stencil;
+        T ko_term = T(0);
+        ko_term += kreiss_oliger<order, dir::x>(arr, comp, idx, geom);
+        ko_term += kreiss_oliger<order, dir::y>(arr, comp, idx, geom);
+        ko_term += kreiss_oliger<order, dir::z>(arr, comp, idx, geom);
+        return T(rhs.template operator()<comp>(idx, time, arr, geom, ws)) + T(strength) * ko_term;
+    }
+
+    /// The decorator is linear, so its linear part decorates the inner linear part.
+    KODecorator linear_part() const
+        requires is_affine_autonomous
+    {
+        return KODecorator{linear_part_of(rhs), strength};
+    }
+
+    RHSType rhs;
+    amrex::Real strength;
+};
+
+static_assert(RHSConcept<KODecorator<NoOpRHS<1, 1>>>);
+
+} // namespace treesap
