@@ -26,17 +26,21 @@
 namespace treesap {
 
 namespace detail {
-/// Tile shape of the fused stage kernel for a given value type, ghost width and component
-/// count: 32-wide rows (one warp), the tallest tile whose ring of shared-memory planes
-/// leaves room for two CTAs per SM, falling back to one CTA per SM for many components.
+/// Tile shape of the fused stage kernel for a value type, ghost width and component count:
+/// 32-wide rows (one warp each), up to 7 rows plus the producer warp (256 threads, two CTAs
+/// per SM within the register file), and the deepest plane ring (prefetch distance P <= 4)
+/// that leaves room for two CTAs per SM; fewer rows and one CTA per SM for many components.
 template <typename T, int G, int NC> struct DefaultTile {
-    template <int TY, int P> using C = treesap_b200::TileCfg<32, TY, G, NC, T, P>;
+    template <int TY, int P, int MINB = 2> using C = treesap_b200::TileCfg<32, TY, G, NC, T, P, MINB>;
     static constexpr int kTwoPerSM = 113 * 1024, kOnePerSM = 220 * 1024;
     using type = std::conditional_t<
-        (C<8, 2>::SMEM <= kTwoPerSM), C<8, 2>,
-        std::conditional_t<(C<4, 2>::SMEM <= kTwoPerSM), C<4, 2>,
-                           std::conditional_t<(C<8, 1>::SMEM <= kOnePerSM), C<8, 1>,
-                                              std::conditional_t<(C<4, 1>::SMEM <= kOnePerSM), C<4, 1>, C<2, 1>>>>>;
+        (C<7, 4>::SMEM <= kTwoPerSM), C<7, 4>,
+        std::conditional_t<
+            (C<7, 3>::SMEM <= kTwoPerSM), C<7, 3>,
+            std::conditional_t<(C<7, 2>::SMEM <= kTwoPerSM), C<7, 2>,
+                               std::conditional_t<(C<3, 2>::SMEM <= kTwoPerSM), C<3, 2>,
+                                                  std::conditional_t<(C<3, 1, 1>::SMEM <= kOnePerSM), C<3, 1, 1>,
+                                                                     C<1, 1, 1>>>>>>;
 };
 } // namespace detail
 
@@ -142,6 +146,13 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
         if (!dst_on_device) treesap_b200::cuda_check(cudaStreamSynchronize(stream()), "cudaStreamSynchronize");
     }
 
+    /// Launch-shape overrides for the fused stage kernels (0 = automatic): tile rows
+    /// (consumer warps per CTA) and the number of z chunks. Used by the autotuner.
+    void set_launch_shape(int rows, int chunks) {
+        tile_rows = rows;
+        z_chunks = chunks;
+    }
+
     /// Kernel launches enqueued by the last step() (for launch accounting).
     long long launches_per_step() const { return launches_per_step_; }
 
@@ -199,6 +210,8 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
     treesap_b200::TensorMapCache tmaps;
     long long launches_per_step_ = 0;
     bool dry_run_ = false; // true while step_host_only() runs: no kernel launches
+    int tile_rows = 0;     // 0: chosen per launch (engine/stage_kernel.cuh choose_ty)
+    int z_chunks = 0;      // 0: chosen per launch (make_shape)
 
   private:
     std::optional<PlotExporter> exporter = std::nullopt;

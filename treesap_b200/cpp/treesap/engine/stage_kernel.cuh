@@ -1,31 +1,40 @@
 // treesap-b200 engine: the fused RK/Euler stage kernel.
 //
-// One launch evaluates one stage of the integrator over the whole box. Each CTA owns an
-// x-y tile of TX x TY cells (one thread per cell, a warp per x row) and marches along z
-// over one or two contiguous z segments (a balanced split of tile-major work across a
-// grid sized to the resident CTA slots). Per z plane:
+// One launch evaluates one stage of the integrator over the whole box. The grid is
+// (x-y tiles) x (z chunks), z-major: CTA b owns tile b % ntiles and z chunk b / ntiles, so the
+// CTAs resident at any time hold neighbouring tiles at the same z and their halo re-reads hit
+// in L2. A CTA has TY consumer warps (one 32-cell x row each, TY <= TYMAX chosen at launch) and
+// one producer warp. Per z plane:
 //
-//   * TMA (cp.async.bulk.tensor.4d, no multicast) copies the plane's tile plus its ghost
-//     halo, all components, into a ring of R shared-memory slots (box (TX+2*XH) x (TY+2G) x 1 x NC,
-//     zero fill outside the array); one mbarrier per slot, a single elected producer thread.
-//   * Each thread keeps its column's values at z-G .. z+G in registers (a queue shifted
-//     once per plane and fed from the newest plane in shared memory).
-//   * The user's RHS functor is called once per component, in component order, on an
-//     Array4 whose StencilView resolves every access at compile time: same-z offsets to
-//     the shared-memory plane, same-column offsets to the register queue, anything else
+//   * the producer warp's elected lane copies the plane's tile plus its ghost halo, all
+//     components, with one TMA load (cp.async.bulk.tensor.4d, no multicast; box
+//     (TX+2*XH) x (TY+2G) x 1 x NC, zero fill outside the array) into a ring of R shared-memory
+//     slots. Slot s has a `full` mbarrier (TMA transaction count) and an `empty` mbarrier
+//     (one arrival per consumer warp); the producer refills a slot once every consumer warp
+//     has released it, running up to R - G - 1 planes ahead of the computation.
+//   * each consumer thread keeps its column's values at z-G .. z+G in a register queue,
+//     shifted once per plane and fed from the newest plane.
+//   * the user's RHS functor is called once per component, in component order, on an Array4
+//     whose StencilView resolves every access at compile time: same-z offsets to the
+//     shared-memory plane, same-column offsets to the register queue, anything else
 //     (mixed x-z / y-z derivatives) to global memory.
-//   * An epilogue policy combines the stage values with the register state and stores
-//     the results (stage accumulator, next-stage argument, ...) with coalesced stores.
+//   * an epilogue policy combines the stage values with centre operands loaded one plane
+//     ahead (register double buffer) and stores the results with coalesced stores.
 //
-// Ring bookkeeping: the planes of a segment are streamed in order; plane `it` (local
-// index, z = z_begin - G + it) is consumed by the queue at iteration it and, when it
-// lies in the segment, by the x-y stencil taps at iteration it + G. A slot is handed
-// back to the producer after a CTA barrier once its plane is no longer needed, so the
-// loads run up to R - G - 1 planes ahead of the computation.
+// No CTA-wide barrier in the plane loop: warps proceed independently, bounded only by the
+// ring. Every wait is bounded (ptx.cuh); on a timeout the kernel records an error bit, lets
+// in-flight copies land and returns.
+//
+// Ring bookkeeping (per chunk, plane index it = 0 .. NP-1, z = z0 - G + it): plane it feeds the
+// queue at iteration it and, when z0 <= z < z1, the x-y stencil taps at iteration it + G. After
+// iteration it a consumer warp has released planes [0, released(it)):
+//   released(it) = it + 1 (it < G),  G (G <= it < 2G),  it - G + 1 (it >= 2G),  NP (last).
 #pragma once
 
 #include <AMReX.H>
 #include <cuda.h>
+
+#include <cmath>
 #include <cuda_runtime.h>
 
 #include "../util/static_for.hpp"
@@ -34,180 +43,160 @@
 
 namespace treesap_b200 {
 
-template <int TX_, int TY_, int G_, int NC_, typename T_, int P_ = 2> struct TileCfg {
+template <int TX_, int TYMAX_, int G_, int NC_, typename T_, int P_ = 2, int MINB_ = 2> struct TileCfg {
     using T = T_;
-    static constexpr int TX = TX_, TY = TY_, G = G_, NC = NC_, P = P_;
-    static constexpr int A = 16 / int(sizeof(T)); // elements per 16 bytes
-    static constexpr int XH = (G + A - 1) / A * A; // x halo width in shared memory (16-byte aligned)
+    static constexpr int TX = TX_, TYMAX = TYMAX_, G = G_, NC = NC_, P = P_;
+    static constexpr int MIN_BLOCKS = MINB_; // resident CTAs per SM the register budget is sized for
+    static constexpr int A = 16 / int(sizeof(T));   // elements per 16 bytes
+    static constexpr int XH = (G + A - 1) / A * A;  // x halo width in shared memory (16-byte aligned)
     static constexpr int BX = TX + 2 * XH;
-    static constexpr int BY = TY + 2 * G;
-    static constexpr int PLANE = NC * BY * BX; // elements per slot
-    static constexpr int R = G + 1 + P;        // ring slots
-    static constexpr int THREADS = TX * TY;
-    static constexpr int SLOT_BYTES = (PLANE * int(sizeof(T)) + 127) / 128 * 128;
-    static constexpr int SMEM = R * SLOT_BYTES + 8 * R;
-    static_assert(TX % A == 0, "tile width must be a multiple of 16 bytes");
-    static_assert(BX <= 256 && BY <= 256 && NC <= 256, "TMA box dimensions are limited to 256");
+    static constexpr int BYMAX = TYMAX + 2 * G;
+    static constexpr int PLANE_MAX = NC * BYMAX * BX; // elements per slot (at TYMAX)
+    static constexpr int R = G + 1 + P;               // ring slots
+    static constexpr int THREADS = TX * TYMAX + 32;   // consumer warps + one producer warp
+    static constexpr int SLOT_BYTES = (PLANE_MAX * int(sizeof(T)) + 127) / 128 * 128;
+    static constexpr int SMEM = R * SLOT_BYTES + 16 * R;
+    static_assert(TX == 32, "one warp per tile row");
+    static_assert(BX <= 256 && BYMAX <= 256 && NC <= 256, "TMA box dimensions are limited to 256");
     static_assert(THREADS <= 1024, "too many threads");
 };
 
 /// Launch-invariant stage inputs.
 template <typename T> struct StageParams {
-    const T* in;               // stencil input field (global fallback for mixed x-z / y-z taps)
-    Layout L;                  // its layout
-    amrex::GeometryData geom;  // passed to the RHS
-    double time;               // stage time t + c_s dt
-    int ntx, nty;              // tiles in x and y
-    long long work;            // ntx * nty * n[2] plane-cells of work
-    int* err;                  // device error word
+    const T* in;              // stencil input field (global fallback for mixed x-z / y-z taps)
+    Layout L;                 // its layout
+    amrex::GeometryData geom; // passed to the RHS
+    double time;              // stage time t + c_s dt
+    int ntx, nty;             // tiles in x and y
+    int ty;                   // tile height (rows = consumer warps), <= TYMAX
+    int zchunk;               // planes per z chunk
+    int* err;                 // device error word
 };
 
 template <class Cfg, class RHS, class Epi>
-__global__ void __launch_bounds__(Cfg::THREADS)
+__global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
     stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageParams<typename Cfg::T> sp, const RHS rhs,
                  const typename Epi::Params ep) {
     using T = typename Cfg::T;
-    constexpr int G = Cfg::G, NC = Cfg::NC, TX = Cfg::TX, BX = Cfg::BX, BY = Cfg::BY, R = Cfg::R, XH = Cfg::XH;
+    constexpr int G = Cfg::G, NC = Cfg::NC, TX = Cfg::TX, BX = Cfg::BX, R = Cfg::R, XH = Cfg::XH;
     constexpr int SLOT = Cfg::SLOT_BYTES / int(sizeof(T));
-    constexpr int PNS = BY * BX; // component stride inside a slot
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
     T* ring = reinterpret_cast<T*>(smem_raw);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + R * Cfg::SLOT_BYTES);
+    uint64_t* empty = full + R;
 
-    const int nz = sp.L.n[2];
-    const long long W = sp.work;
-    const long long wb = W * blockIdx.x / gridDim.x, we = W * (blockIdx.x + 1) / gridDim.x;
-    if (wb >= we) return;
-
-    // Segments of this CTA: maximal runs of [wb, we) inside one tile column.
-    // Plane stream: segment by segment, planes z_b - G .. z_e - 1 + G.
-    auto seg_tile = [&](long long w) { return int(w / nz); };
-    long long total_planes = 0;
-    for (long long w = wb; w < we;) {
-        const long long wend = (w / nz + 1) * nz < we ? (w / nz + 1) * nz : we;
-        total_planes += (wend - w) + 2 * G;
-        w = wend;
-    }
+    const int TY = sp.ty;
+    const int BY = TY + 2 * G;
+    const int PNS = BY * BX; // component stride inside a slot
+    const int ntiles = sp.ntx * sp.nty;
+    const int tile = blockIdx.x % ntiles;
+    const int z0 = (blockIdx.x / ntiles) * sp.zchunk;
+    const int z1 = min(sp.L.n[2], z0 + sp.zchunk);
+    if (z0 >= z1) return;
+    const int NP = (z1 - z0) + 2 * G; // planes streamed: z0 - G .. z1 - 1 + G
+    const int x0 = (tile % sp.ntx) * TX, y0 = (tile / sp.ntx) * TY;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
 
     if (threadIdx.x == 0) {
-        ptx::prefetch_tensor_map(&tmap);
-        for (int s = 0; s < R; ++s) ptx::mbar_init(&full[s], 1);
+        for (int s = 0; s < R; ++s) {
+            ptx::mbar_init(&full[s], 1);
+            ptx::mbar_init(&empty[s], uint32_t(TY));
+        }
         ptx::fence_mbar_init();
     }
     __syncthreads();
 
-    // Producer state (thread 0 only): the stream is re-derived from (segment, local index).
-    long long issued = 0;
-    long long prod_w = wb; // segment cursor of the producer
-    int prod_it = 0;       // local plane index inside the producer's segment
-    auto issue_upto = [&](long long limit) {
-        while (issued < limit && issued < total_planes) {
-            const int tile = seg_tile(prod_w);
-            const int zb = int(prod_w % nz);
-            const long long sege = ((prod_w / nz) + 1) * nz < we ? ((prod_w / nz) + 1) * nz : we;
-            const int nplanes = int(sege - prod_w) + 2 * G;
-            const int s = int(issued % R);
-            const int x0 = (tile % sp.ntx) * TX, y0 = (tile / sp.ntx) * Cfg::TY;
-            ptx::mbar_arrive_expect_tx(&full[s], uint32_t(Cfg::PLANE * sizeof(T)));
-            // storage coordinates: x = x0 - XH + xoff (= x0), y = y0 - G + g (= y0), z = zb - G + it + g
-            ptx::tma_load_4d(ring + s * SLOT, &tmap, x0, y0, zb + prod_it, 0, &full[s]);
-            ++issued;
-            if (++prod_it == nplanes) {
-                prod_it = 0;
-                prod_w = sege;
+    if (warp == TY) {
+        // ---------------------------------------------------------------- producer warp
+        if (lane == 0) {
+            ptx::prefetch_tensor_map(&tmap);
+            const uint32_t bytes = uint32_t(NC * BY * BX * int(sizeof(T)));
+            int q = 0;
+            for (; q < NP; ++q) {
+                const int s = q % R;
+                if (q >= R && !ptx::mbar_wait(&empty[s], uint32_t(((q / R) - 1) & 1), sp.err)) break;
+                ptx::mbar_arrive_expect_tx(&full[s], bytes);
+                // storage coordinates: x = x0 - XH + xoff (= x0), y = y0 - G + g (= y0), z = z0 - G + q + g
+                ptx::tma_load_4d(ring + s * SLOT, &tmap, x0, y0, z0 + q, 0, &full[s]);
+            }
+            if (q < NP) {
+                // a consumer warp stopped releasing slots: let the copies in flight land
+                for (int r = (q > R ? q - R : 0); r < q; ++r)
+                    ptx::mbar_wait(&full[r % R], uint32_t((r / R) & 1), nullptr, 100000000ull);
             }
         }
-    };
-    if (threadIdx.x == 0) issue_upto(R);
+        return;
+    }
+    if (warp > TY) return;
 
-    const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+    // -------------------------------------------------------------------- consumer warps
+    const int tx = lane, ty = warp;
+    const int i = x0 + tx, j = y0 + ty;
+    const bool active = (i < sp.L.n[0]) && (j < sp.L.n[1]);
     const int coff = (ty + G) * BX + (tx + XH); // this thread's centre inside a slot
 
     T q[(2 * G + 1) * NC]; // register queue: q[(dk + G) * NC + c]
 #pragma unroll
     for (int e = 0; e < (2 * G + 1) * NC; ++e) q[e] = T(0);
 
-    long long consumed = 0; // planes fully released (slot handed back)
-    long long streamed = 0; // planes consumed by the queue so far (global stream index)
-    bool failed = false;
+    using Pre = typename Epi::template Pre<NC>;
+    Pre pre{};
+    if (active) pre = Epi::template load<NC>(ep, i, j, z0);
 
-    for (long long w = wb; w < we && !failed;) {
-        const int tile = seg_tile(w);
-        const int zb = int(w % nz);
-        const long long sege = ((w / nz) + 1) * nz < we ? ((w / nz) + 1) * nz : we;
-        const int nplanes = int(sege - w) + 2 * G;
-        const long long seg_base = streamed;
-        const int i = (tile % sp.ntx) * TX + tx;
-        const int j = (tile / sp.ntx) * Cfg::TY + ty;
-        const bool active = (i < sp.L.n[0]) && (j < sp.L.n[1]);
-
-        for (int it = 0; it < nplanes; ++it) {
-            const long long gq = seg_base + it;
-            const int s = int(gq % R);
-            if (!ptx::mbar_wait(&full[s], uint32_t((gq / R) & 1), sp.err)) failed = true;
-            if (!failed) {
-                const T* slot = ring + s * SLOT;
+    int released = 0;
+    for (int it = 0; it < NP; ++it) {
+        const int s = it % R;
+        if (!ptx::mbar_wait(&full[s], uint32_t((it / R) & 1), sp.err)) break;
+        const T* slot = ring + s * SLOT;
 #pragma unroll
-                for (int e = 0; e < 2 * G * NC; ++e) q[e] = q[e + NC];
+        for (int e = 0; e < 2 * G * NC; ++e) q[e] = q[e + NC];
 #pragma unroll
-                for (int c = 0; c < NC; ++c) q[2 * G * NC + c] = slot[c * PNS + coff];
+        for (int c = 0; c < NC; ++c) q[2 * G * NC + c] = slot[c * PNS + coff];
 
-                if (it >= 2 * G && active) {
-                    const int z = zb - 2 * G + it;
-                    const T* ctr = ring + int((gq - G) % R) * SLOT + coff;
-                    amrex::StencilView<T> view{ctr,
-                                               q,
-                                               sp.in + sp.L.index(i, j, z, 0),
-                                               sp.L.px,
-                                               sp.L.px * sp.L.py,
-                                               sp.L.comp_stride(),
-                                               i,
-                                               j,
-                                               z,
-                                               BX,
-                                               PNS,
-                                               G,
-                                               NC};
-                    amrex::Array4<const T> arr = make_array4<const T>(sp.in, sp.L);
-                    arr.view = &view;
-                    typename RHS::Workspace ws{};
-                    T kv[NC];
-                    const amrex::IntVect idx{i, j, z};
-                    treesap::static_for<NC>([&]<int c>() {
-                        kv[c] = static_cast<T>(rhs.template operator()<c>(idx, sp.time, arr, sp.geom, ws));
-                    });
-                    Epi::template apply<T, NC>(ep, kv, ctr, PNS, i, j, z);
-                }
-            }
-            streamed = gq + 1;
-            // release: planes below z_b are only queue inputs; planes inside the segment are
-            // released after their x-y taps were used (G iterations after they arrived)
-            long long released = seg_base + (it < G ? it + 1 : (it < 2 * G ? G : it - G + 1));
-            if (it == nplanes - 1) released = seg_base + nplanes;
-            if (__syncthreads_or(failed)) {
-                failed = true;
-                break;
-            }
-            if (threadIdx.x == 0) {
-                ptx::fence_proxy_async_smem();
-                consumed = released;
-                issue_upto(consumed + R);
-            }
+        if (it >= 2 * G && active) {
+            const int z = z0 - 2 * G + it;
+            Pre pre_next{};
+            if (z + 1 < z1) pre_next = Epi::template load<NC>(ep, i, j, z + 1);
+            const T* ctr = ring + ((it - G) % R) * SLOT + coff;
+            amrex::StencilView<T> view{ctr,
+                                       q,
+                                       sp.in + sp.L.index(i, j, z, 0),
+                                       sp.L.px,
+                                       sp.L.px * sp.L.py,
+                                       sp.L.comp_stride(),
+                                       i,
+                                       j,
+                                       z,
+                                       BX,
+                                       PNS,
+                                       G,
+                                       NC};
+            amrex::Array4<const T> arr = make_array4<const T>(sp.in, sp.L);
+            arr.view = &view;
+            typename RHS::Workspace ws{};
+            T kv[NC];
+            const amrex::IntVect idx{i, j, z};
+            treesap::static_for<NC>([&]<int c>() {
+                kv[c] = static_cast<T>(rhs.template operator()<c>(idx, sp.time, arr, sp.geom, ws));
+            });
+            Epi::template apply<T, NC>(ep, kv, ctr, PNS, i, j, z, pre);
+            pre = pre_next;
         }
-        w = sege;
-    }
-
-    if (failed && threadIdx.x == 0) {
-        // Let copies still in flight land before the CTA's shared memory is released.
-        for (long long gq = streamed; gq < issued; ++gq)
-            ptx::mbar_wait(&full[int(gq % R)], uint32_t((gq / R) & 1), sp.err, 100000000ull);
+        int rel = (it < G) ? it + 1 : (it < 2 * G ? G : it - G + 1);
+        if (it == NP - 1) rel = NP;
+        __syncwarp();
+        if (lane == 0)
+            for (int r = released; r < rel; ++r) ptx::mbar_arrive(&empty[r % R]);
+        released = rel;
     }
 }
 
 // ------------------------------------------------------------------ epilogues
-// Each policy: struct Params; template <T, NC> static void apply(params, k[NC], centre, pns, i, j, z)
-// where `centre` points at component 0 of the stencil input's centre in shared memory.
+// Each policy: struct Params; struct Pre (centre operands loaded one plane ahead);
+// static Pre load(params, i, j, z); template <T, NC> static void apply(params, k[NC], centre,
+// pns, i, j, z, pre) where `centre` points at component 0 of the stencil input's centre in
+// shared memory.
 
 /// FP64 plain RK4 stage s with the reference's register scheme
 /// (integrators/SingleLevelRK4Integrator.hpp:139-155):
@@ -222,24 +211,36 @@ template <int STAGE> struct EpiRK4 {
         Layout L;
         double b, a_next;
     };
+    template <int NC> struct Pre {
+        double acc[NC];
+        double init[NC];
+    };
+    template <int NC> static __device__ __forceinline__ Pre<NC> load(const Params& p, int i, int j, int z) {
+        Pre<NC> r;
+        if constexpr (STAGE > 0) {
+            const long long o0 = p.L.index(i, j, z, 0), cs = p.L.comp_stride();
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                r.acc[c] = __ldcs(p.acc + o0 + c * cs);
+                if constexpr (STAGE < 3) r.init[c] = __ldg(p.init + o0 + c * cs);
+            }
+        }
+        return r;
+    }
     template <class T, int NC>
     static __device__ __forceinline__ void apply(const Params& p, const T (&k)[NC], const T* centre, int pns, int i,
-                                                 int j, int z) {
+                                                 int j, int z, const Pre<NC>& pre) {
         const long long o0 = p.L.index(i, j, z, 0), cs = p.L.comp_stride();
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
             const long long o = o0 + c * cs;
             if constexpr (STAGE == 0) {
                 const double u0 = centre[c * pns];
-                p.acc[o] = u0 + p.b * k[c];
-                p.arg_next[o] = u0 + p.a_next * k[c];
+                __stcs(p.acc + o, u0 + p.b * k[c]);
+                __stcs(p.arg_next + o, u0 + p.a_next * k[c]);
             } else {
-                const double a0 = p.acc[o];
-                if constexpr (STAGE < 3) {
-                    const double u0 = __ldg(p.init + o);
-                    p.arg_next[o] = u0 + p.a_next * k[c];
-                }
-                p.acc[o] = a0 + p.b * k[c];
+                if constexpr (STAGE < 3) __stcs(p.arg_next + o, pre.init[c] + p.a_next * k[c]);
+                __stcs(p.acc + o, pre.acc[c] + p.b * k[c]);
             }
         }
     }
@@ -252,12 +253,14 @@ struct EpiEuler {
         Layout L;
         double dt;
     };
+    template <int NC> struct Pre {};
+    template <int NC> static __device__ __forceinline__ Pre<NC> load(const Params&, int, int, int) { return {}; }
     template <class T, int NC>
     static __device__ __forceinline__ void apply(const Params& p, const T (&k)[NC], const T* centre, int pns, int i,
-                                                 int j, int z) {
+                                                 int j, int z, const Pre<NC>&) {
         const long long o0 = p.L.index(i, j, z, 0), cs = p.L.comp_stride();
 #pragma unroll
-        for (int c = 0; c < NC; ++c) p.out[o0 + c * cs] = centre[c * pns] + p.dt * k[c];
+        for (int c = 0; c < NC; ++c) __stcs(p.out + o0 + c * cs, centre[c * pns] + p.dt * k[c]);
     }
 };
 
@@ -273,9 +276,11 @@ struct EpiF32S0 {
         float* k0;
         Layout Lf;
     };
+    template <int NC> struct Pre {};
+    template <int NC> static __device__ __forceinline__ Pre<NC> load(const Params&, int, int, int) { return {}; }
     template <class T, int NC>
-    static __device__ __forceinline__ void apply(const Params& p, const T (&k)[NC], const T*, int, int i, int j,
-                                                 int z) {
+    static __device__ __forceinline__ void apply(const Params& p, const T (&k)[NC], const T*, int, int i, int j, int z,
+                                                 const Pre<NC>&) {
         const long long o0 = p.Lf.index(i, j, z, 0), cs = p.Lf.comp_stride();
 #pragma unroll
         for (int c = 0; c < NC; ++c) p.k0[o0 + c * cs] = static_cast<float>(k[c]);
@@ -293,28 +298,44 @@ template <int STAGE> struct EpiF32Lin {
         float a_dt;         // a_s dt
         double dt;          // stage 3
     };
+    template <int NC> struct Pre {
+        float k0[NC], k1[NC];
+        double u[NC];
+    };
+    template <int NC> static __device__ __forceinline__ Pre<NC> load(const Params& p, int i, int j, int z) {
+        Pre<NC> r;
+        if constexpr (STAGE >= 2) {
+            const long long o0 = p.Lf.index(i, j, z, 0), cs = p.Lf.comp_stride();
+            const long long u0 = p.Lu.index(i, j, z, 0), us = p.Lu.comp_stride();
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                r.k0[c] = __ldcs(p.k0 + o0 + c * cs);
+                if constexpr (STAGE == 3) {
+                    r.k1[c] = __ldcs(p.k1 + o0 + c * cs);
+                    r.u[c] = __ldcs(p.u_in + u0 + c * us);
+                }
+            }
+        }
+        return r;
+    }
     template <class T, int NC>
     static __device__ __forceinline__ void apply(const Params& p, const T (&lk)[NC], const T* centre, int pns, int i,
-                                                 int j, int z) {
+                                                 int j, int z, const Pre<NC>& pre) {
         const long long o0 = p.Lf.index(i, j, z, 0), cs = p.Lf.comp_stride();
         if constexpr (STAGE == 1) {
 #pragma unroll
             for (int c = 0; c < NC; ++c) p.k_out[o0 + c * cs] = centre[c * pns] + p.a_dt * lk[c];
         } else if constexpr (STAGE == 2) {
 #pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                const long long o = o0 + c * cs;
-                p.k_out[o] = __ldg(p.k0 + o) + p.a_dt * lk[c];
-            }
+            for (int c = 0; c < NC; ++c) p.k_out[o0 + c * cs] = pre.k0[c] + p.a_dt * lk[c];
         } else {
             const long long u0 = p.Lu.index(i, j, z, 0), us = p.Lu.comp_stride();
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
-                const long long o = o0 + c * cs;
-                const float k0 = __ldg(p.k0 + o), k1 = __ldg(p.k1 + o), k2 = centre[c * pns];
-                const float k3 = k0 + p.a_dt * lk[c];
-                const double sum = double(k0) + 2.0 * double(k1) + 2.0 * double(k2) + double(k3);
-                p.u[u0 + c * us] = __ldg(p.u_in + u0 + c * us) + (p.dt / 6.0) * sum;
+                const float k2 = centre[c * pns];
+                const float k3 = pre.k0[c] + p.a_dt * lk[c];
+                const double sum = double(pre.k0[c]) + 2.0 * double(pre.k1[c]) + 2.0 * double(k2) + double(k3);
+                __stcs(p.u + u0 + c * us, pre.u[c] + (p.dt / 6.0) * sum);
             }
         }
     }
@@ -323,23 +344,47 @@ template <int STAGE> struct EpiF32Lin {
 // ------------------------------------------------------------------ host launch
 struct LaunchShape {
     int grid = 0;
-    int ntx = 0, nty = 0;
-    long long work = 0;
+    int ntx = 0, nty = 0, ty = 0;
+    int nchunks = 0, zchunk = 0;
 };
 
-/// Grid size: one CTA per resident slot (occupancy x SMs), but no CTA with less than
-/// `min_planes` planes of work (short segments pay 2G warm-up planes each).
-template <class Cfg> LaunchShape make_shape(const Layout& L, int slots) {
+/// z-major grid: tiles of 32 x ty cells, the z extent split into `nchunks` chunks so that the
+/// grid fills the resident CTA slots without chunks shorter than 4G planes (each chunk pays a
+/// 2G-plane warm-up).
+template <class Cfg> LaunchShape make_shape(const Layout& L, int slots, int ty, int nchunks = 0) {
     LaunchShape s;
+    s.ty = ty;
     s.ntx = (L.n[0] + Cfg::TX - 1) / Cfg::TX;
-    s.nty = (L.n[1] + Cfg::TY - 1) / Cfg::TY;
-    s.work = (long long)s.ntx * s.nty * L.n[2];
-    const long long min_planes = 8 * Cfg::G > 16 ? 8 * Cfg::G : 16;
-    long long g = (s.work + min_planes - 1) / min_planes;
-    if (g > slots) g = slots;
-    if (g < 1) g = 1;
-    s.grid = int(g);
+    s.nty = (L.n[1] + ty - 1) / ty;
+    const int ntiles = s.ntx * s.nty;
+    if (nchunks <= 0) {
+        nchunks = slots / ntiles;
+        const int min_chunk = 4 * Cfg::G > 8 ? 4 * Cfg::G : 8;
+        const int max_chunks = L.n[2] / min_chunk > 1 ? L.n[2] / min_chunk : 1;
+        if (nchunks > max_chunks) nchunks = max_chunks;
+        if (nchunks < 1) nchunks = 1;
+    }
+    s.zchunk = (L.n[2] + nchunks - 1) / nchunks;
+    s.nchunks = (L.n[2] + s.zchunk - 1) / s.zchunk;
+    s.grid = ntiles * s.nchunks;
     return s;
+}
+
+/// Tile height for a given width in x: the largest ty <= TYMAX whose tile count fills the SMs
+/// most evenly (fraction of busy slot-time in the last wave), ties to the taller tile.
+template <class Cfg> int choose_ty(const Layout& L, int slots) {
+    int best = Cfg::TYMAX;
+    double best_eff = -1.0;
+    for (int ty = Cfg::TYMAX; ty >= (Cfg::TYMAX + 1) / 2; --ty) {
+        const LaunchShape s = make_shape<Cfg>(L, slots, ty);
+        const double waves = double(s.grid) / slots;
+        const double eff = waves / std::ceil(waves) * (double(ty) / Cfg::TYMAX > 0.75 ? 1.0 : 0.95);
+        if (eff > best_eff + 1e-9) {
+            best_eff = eff;
+            best = ty;
+        }
+    }
+    return best;
 }
 
 template <class Cfg, class RHS, class Epi> struct StageLauncher {
@@ -360,13 +405,23 @@ template <class Cfg, class RHS, class Epi> struct StageLauncher {
         }
         return occ[dev];
     }
+    /// Launch shape for a layout; `ty` <= 0 picks the tile height, `nchunks` <= 0 the z split.
+    static LaunchShape shape(const Layout& L, int sm_count, int ty = 0, int nchunks = 0) {
+        const int slots = occupancy() * sm_count;
+        if (ty <= 0 || ty > Cfg::TYMAX) ty = choose_ty<Cfg>(L, slots);
+        return make_shape<Cfg>(L, slots, ty, nchunks);
+    }
+    /// The TMA box of a launch shape: (TX + 2 XH) x (ty + 2G).
+    static int box_x() { return Cfg::BX; }
+    static int box_y(const LaunchShape& s) { return s.ty + 2 * Cfg::G; }
     static void launch(const CUtensorMap& tmap, StageParams<typename Cfg::T> sp, const RHS& rhs,
-                       const typename Epi::Params& ep, int sm_count, cudaStream_t stream) {
-        const LaunchShape s = make_shape<Cfg>(sp.L, occupancy() * sm_count);
+                       const typename Epi::Params& ep, const LaunchShape& s, cudaStream_t stream) {
         sp.ntx = s.ntx;
         sp.nty = s.nty;
-        sp.work = s.work;
-        stage_kernel<Cfg, RHS, Epi><<<s.grid, Cfg::THREADS, Cfg::SMEM, stream>>>(tmap, sp, rhs, ep);
+        sp.ty = s.ty;
+        sp.zchunk = s.zchunk;
+        const int threads = 32 * s.ty + 32;
+        stage_kernel<Cfg, RHS, Epi><<<s.grid, threads, Cfg::SMEM, stream>>>(tmap, sp, rhs, ep);
         cuda_check(cudaGetLastError(), "stage_kernel launch");
     }
 };

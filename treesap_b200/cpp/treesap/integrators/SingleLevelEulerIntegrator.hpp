@@ -35,10 +35,10 @@ class SingleLevelEulerIntegrator : public SingleLevelIntegrator<PDEModelType> {
         sp.time = time;
         sp.err = ts_context_error_word(this->ctx);
         treesap_b200::EpiEuler::Params ep{state_new.data(), L, delta_time};
-        const CUtensorMap& tm = this->tensor_map(state_old.data(), L, TS_F64, Tile::BX, Tile::BY);
-        if (!this->dry_run_)
-            treesap_b200::StageLauncher<Tile, RHSType, treesap_b200::EpiEuler>::launch(tm, sp, model.get_rhs(), ep,
-                                                                                   this->sm_count(), this->stream());
+        using Launcher = treesap_b200::StageLauncher<Tile, RHSType, treesap_b200::EpiEuler>;
+        const auto shape = Launcher::shape(L, this->sm_count(), this->tile_rows, this->z_chunks);
+        const CUtensorMap& tm = this->tensor_map(state_old.data(), L, TS_F64, Launcher::box_x(), Launcher::box_y(shape));
+        if (!this->dry_run_) Launcher::launch(tm, sp, model.get_rhs(), ep, shape, this->stream());
         this->launches_per_step_ = 2;
         return delta_time;
     }

@@ -66,9 +66,10 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
             sp.time = time;
             sp.err = err;
             EpiF32S0::Params ep{k0.data(), Lf};
-            StageLauncher<Tile64, RHSType, EpiF32S0>::launch(
-                this->tensor_map(state_old.data(), Lu, TS_F64, Tile64::BX, Tile64::BY), sp, model.get_rhs(), ep,
-                this->sm_count(), this->stream());
+            using Launcher = StageLauncher<Tile64, RHSType, EpiF32S0>;
+            const auto shape = Launcher::shape(Lu, this->sm_count(), this->tile_rows, this->z_chunks);
+            Launcher::launch(this->tensor_map(state_old.data(), Lu, TS_F64, Launcher::box_x(), Launcher::box_y(shape)),
+                             sp, model.get_rhs(), ep, shape, this->stream());
         }
         fill_increment(k0);
         lin_stage<1>(k0, k1, float(0.5 * dt), dt, err);
@@ -99,9 +100,10 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
         ep.Lu = state_old.layout();
         ep.a_dt = a_dt;
         ep.dt = dt;
-        StageLauncher<Tile32, LinearRHS, EpiF32Lin<S>>::launch(
-            this->tensor_map(in.data(), Lf, TS_F32, Tile32::BX, Tile32::BY), sp, lin, ep, this->sm_count(),
-            this->stream());
+        using Launcher = StageLauncher<Tile32, LinearRHS, EpiF32Lin<S>>;
+        const auto shape = Launcher::shape(Lf, this->sm_count(), this->tile_rows, this->z_chunks);
+        Launcher::launch(this->tensor_map(in.data(), Lf, TS_F32, Launcher::box_x(), Launcher::box_y(shape)), sp, lin,
+                         ep, shape, this->stream());
     }
 
     void fill_increment(FieldF& f) {

@@ -68,10 +68,11 @@ class SingleLevelRK4Integrator : public SingleLevelIntegrator<PDEModelType> {
         sp.time = time_arg;
         sp.err = ts_context_error_word(this->ctx);
         typename treesap_b200::EpiRK4<s>::Params ep{state_new.data(), arg_next.data(), state_old.data(), L, b, a_next};
-        const CUtensorMap& tm = this->tensor_map(input.data(), L, TS_F64, Tile::BX, Tile::BY);
+        using Launcher = treesap_b200::StageLauncher<Tile, RHSType, treesap_b200::EpiRK4<s>>;
+        const auto shape = Launcher::shape(L, this->sm_count(), this->tile_rows, this->z_chunks);
+        const CUtensorMap& tm = this->tensor_map(input.data(), L, TS_F64, Launcher::box_x(), Launcher::box_y(shape));
         if (this->dry_run_) return;
-        treesap_b200::StageLauncher<Tile, RHSType, treesap_b200::EpiRK4<s>>::launch(
-            tm, sp, model.get_rhs(), ep, this->sm_count(), this->stream());
+        Launcher::launch(tm, sp, model.get_rhs(), ep, shape, this->stream());
     }
 
     Field arg;
