@@ -155,6 +155,17 @@ TS_API ts_status ts_integrator_use_graph(ts_integrator* it, int enable);
  * context stream (valid after ts_context_sync), and the number of kernels it launched. */
 TS_API ts_status ts_integrator_last_step_timing(ts_integrator* it, double* ms, long long* launches);
 
+/* Runs nsteps steps (like ts_integrator_step) with a CUDA event pair around every kernel
+ * launch, waits, and returns per kernel class c < nclasses the number of launches and their
+ * summed device time in ms. Classes: 0 ghost fill, 1 + s stage s of the step (Euler: 1).
+ * (Instrumentation of Integrator.hpp:91-106 / ScopedTimer.hpp, with device clocks.) */
+TS_API ts_status ts_integrator_profile(ts_integrator* it, int nsteps, int nclasses, long long* launches, double* ms);
+
+/* Overrides the launch shape of the fused stage kernels: rows = tile height (consumer warps
+ * per CTA, 0 = automatic), chunks = number of z chunks (0 = automatic). Used by the autotuner;
+ * the default shape is chosen per launch from the SM count and the domain. */
+TS_API ts_status ts_integrator_set_launch_shape(ts_integrator* it, int rows, int chunks);
+
 #ifdef __cplusplus
 }
 #endif

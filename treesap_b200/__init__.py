@@ -140,6 +140,8 @@ def lib() -> C.CDLL:
         "ts_integrator_state_field": (i, [vp, C.POINTER(vp), C.POINTER(FieldLayout)]),
         "ts_integrator_use_graph": (i, [vp, i]),
         "ts_integrator_last_step_timing": (i, [vp, C.POINTER(d), C.POINTER(ll)]),
+        "ts_integrator_profile": (i, [vp, i, i, C.POINTER(ll), C.POINTER(d)]),
+        "ts_integrator_set_launch_shape": (i, [vp, i, i]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -246,6 +248,16 @@ class Integrator:
         ms, n = C.c_double(), C.c_longlong()
         _check(lib().ts_integrator_last_step_timing(self.handle, C.byref(ms), C.byref(n)), "timing", self.ctx)
         return ms.value, n.value
+
+    def profile(self, nsteps: int, nclasses: int = 5) -> tuple[list[int], list[float]]:
+        """Per kernel class (0 ghost fill, 1+s stage s): launches and total device ms over nsteps steps."""
+        n = (C.c_longlong * nclasses)()
+        ms = (C.c_double * nclasses)()
+        _check(lib().ts_integrator_profile(self.handle, nsteps, nclasses, n, ms), "ts_integrator_profile", self.ctx)
+        return list(n), list(ms)
+
+    def set_launch_shape(self, rows: int = 0, chunks: int = 0) -> None:
+        _check(lib().ts_integrator_set_launch_shape(self.handle, rows, chunks), "set_launch_shape", self.ctx)
 
     def state_field(self) -> tuple[int, FieldLayout]:
         p, L = C.c_void_p(), FieldLayout()

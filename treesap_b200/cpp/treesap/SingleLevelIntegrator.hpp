@@ -25,6 +25,40 @@
 
 namespace treesap {
 
+/// Optional per-launch device clock: when attached to an integrator, every kernel launch is
+/// bracketed by a CUDA event pair on the integrator's stream and tagged with a class
+/// (0 ghost fill, 1 + s for stage s of the step).
+struct KernelClock {
+    struct Span {
+        int cls;
+        cudaEvent_t a, b;
+    };
+    std::vector<Span> spans;
+    void begin(int cls, cudaStream_t s) {
+        Span sp{cls, nullptr, nullptr};
+        treesap_b200::cuda_check(cudaEventCreate(&sp.a), "cudaEventCreate");
+        treesap_b200::cuda_check(cudaEventCreate(&sp.b), "cudaEventCreate");
+        treesap_b200::cuda_check(cudaEventRecord(sp.a, s), "cudaEventRecord");
+        spans.push_back(sp);
+    }
+    void end(cudaStream_t s) { treesap_b200::cuda_check(cudaEventRecord(spans.back().b, s), "cudaEventRecord"); }
+    /// Sums launch counts and milliseconds per class (after the stream has completed).
+    void collect(int nclasses, long long* launches, double* ms) {
+        for (int c = 0; c < nclasses; ++c) launches[c] = 0, ms[c] = 0.0;
+        for (auto& sp : spans) {
+            float f = 0.f;
+            cudaEventElapsedTime(&f, sp.a, sp.b);
+            if (sp.cls >= 0 && sp.cls < nclasses) {
+                launches[sp.cls] += 1;
+                ms[sp.cls] += f;
+            }
+            cudaEventDestroy(sp.a);
+            cudaEventDestroy(sp.b);
+        }
+        spans.clear();
+    }
+};
+
 namespace detail {
 /// Tile shape of the fused stage kernel for a value type, ghost width and component count:
 /// 32-wide rows (one warp each), up to 7 rows plus the producer warp (256 threads, two CTAs
@@ -146,6 +180,9 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
         if (!dst_on_device) treesap_b200::cuda_check(cudaStreamSynchronize(stream()), "cudaStreamSynchronize");
     }
 
+    /// Attach (or detach with nullptr) a per-launch device clock.
+    void attach_clock(KernelClock* c) { clock_ = c; }
+
     /// Launch-shape overrides for the fused stage kernels (0 = automatic): tile rows
     /// (consumer warps per CTA) and the number of z chunks. Used by the autotuner.
     void set_launch_shape(int rows, int chunks) {
@@ -176,8 +213,10 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
     void FillPatch(Field& f, amrex::Real time_) {
         ScopedTimer timer("Integrator::FillPatch()");
         if (dry_run_) return;
+        clock_begin(0);
         treesap_b200::launch_ghost_fill(f.data(), f.layout(), geom, model.get_bc(), bc_recs_dev, time_,
                                         treesap_b200::GhostMode::Functor, sm_count(), stream());
+        clock_end();
     }
 
     const CUtensorMap& tensor_map(const void* base, const treesap_b200::Layout& L, int dtype, int box_x, int box_y) {
@@ -210,6 +249,13 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
     treesap_b200::TensorMapCache tmaps;
     long long launches_per_step_ = 0;
     bool dry_run_ = false; // true while step_host_only() runs: no kernel launches
+    KernelClock* clock_ = nullptr;
+    void clock_begin(int cls) {
+        if (clock_) clock_->begin(cls, stream());
+    }
+    void clock_end() {
+        if (clock_) clock_->end(stream());
+    }
     int tile_rows = 0;     // 0: chosen per launch (engine/stage_kernel.cuh choose_ty)
     int z_chunks = 0;      // 0: chosen per launch (make_shape)
 

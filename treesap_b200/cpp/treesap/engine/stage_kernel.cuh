@@ -131,9 +131,18 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
     if (warp > TY) return;
 
     // -------------------------------------------------------------------- consumer warps
+    // Register copies of everything the plane loop reads: values in kernel-parameter space are
+    // not known to be loop-invariant, which would keep e.g. the stencils' 1/dx factors and the
+    // functor's data inside the loop.
+    const RHS f = rhs;
+    const amrex::GeometryData geom = sp.geom;
+    const Layout L = sp.L;
+    const double time = sp.time;
+    const typename Epi::Params epl = ep;
+
     const int tx = lane, ty = warp;
     const int i = x0 + tx, j = y0 + ty;
-    const bool active = (i < sp.L.n[0]) && (j < sp.L.n[1]);
+    const bool active = (i < L.n[0]) && (j < L.n[1]);
     const int coff = (ty + G) * BX + (tx + XH); // this thread's centre inside a slot
 
     T q[(2 * G + 1) * NC]; // register queue: q[(dk + G) * NC + c]
@@ -142,7 +151,9 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
 
     using Pre = typename Epi::template Pre<NC>;
     Pre pre{};
-    if (active) pre = Epi::template load<NC>(ep, i, j, z0);
+    if (active) pre = Epi::template load<NC>(epl, i, j, z0);
+    const T* in_col = sp.in + L.index(i, j, 0, 0); // global fallback: this column at z = 0
+    const long long plane = L.px * L.py;
 
     int released = 0;
     for (int it = 0; it < NP; ++it) {
@@ -157,30 +168,19 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
         if (it >= 2 * G && active) {
             const int z = z0 - 2 * G + it;
             Pre pre_next{};
-            if (z + 1 < z1) pre_next = Epi::template load<NC>(ep, i, j, z + 1);
+            if (z + 1 < z1) pre_next = Epi::template load<NC>(epl, i, j, z + 1);
             const T* ctr = ring + ((it - G) % R) * SLOT + coff;
-            amrex::StencilView<T> view{ctr,
-                                       q,
-                                       sp.in + sp.L.index(i, j, z, 0),
-                                       sp.L.px,
-                                       sp.L.px * sp.L.py,
-                                       sp.L.comp_stride(),
-                                       i,
-                                       j,
-                                       z,
-                                       BX,
-                                       PNS,
-                                       G,
-                                       NC};
-            amrex::Array4<const T> arr = make_array4<const T>(sp.in, sp.L);
+            amrex::StencilView<T> view{ctr, q, in_col + z * plane, L.px, plane, L.comp_stride(), i, j, z, BX, PNS,
+                                       G, NC};
+            amrex::Array4<const T> arr = make_array4<const T>(sp.in, L);
             arr.view = &view;
             typename RHS::Workspace ws{};
             T kv[NC];
             const amrex::IntVect idx{i, j, z};
             treesap::static_for<NC>([&]<int c>() {
-                kv[c] = static_cast<T>(rhs.template operator()<c>(idx, sp.time, arr, sp.geom, ws));
+                kv[c] = static_cast<T>(f.template operator()<c>(idx, time, arr, geom, ws));
             });
-            Epi::template apply<T, NC>(ep, kv, ctr, PNS, i, j, z, pre);
+            Epi::template apply<T, NC>(epl, kv, ctr, PNS, i, j, z, pre);
             pre = pre_next;
         }
         int rel = (it < G) ? it + 1 : (it < 2 * G ? G : it - G + 1);
@@ -264,56 +264,76 @@ struct EpiEuler {
     }
 };
 
-/// FP32-stage RK4 for affine autonomous right-hand sides F(u) = L u + f0.
-///   stage 0 (FP64 input u):   k0 = F(u)                         -> k0 (FP32)
-///   stage 1 (FP32 input k0):  k1 = k0 + (dt/2) L k0             -> k1
-///   stage 2 (FP32 input k1):  k2 = k0 + (dt/2) L k1             -> k2
-///   stage 3 (FP32 input k2):  k3 = k0 + dt L k2,
-///                             u_new = u + dt/6 (k0 + 2 k1 + 2 k2 + k3)  in FP64
-/// which is algebraically the classical RK4 step k_s = F(u + a_s dt k_{s-1}).
+/// FP32-stage RK4 for affine autonomous right-hand sides F(u) = L u + f0. The stage values
+/// are carried as k0 plus differences d_s = k_s - k0, and every stencil of a full-magnitude
+/// field runs in FP64 (a centred D2 of half-width 4 cancels ~1e6-fold, beyond FP32):
+///   stage 0 (FP64 input u):   k0 = F(u);  u_p = u + dt k0                 -> k0 (FP64), u_p (FP64)
+///   stage 1 (FP64 input k0):  d1 = dt/2 L k0                              -> d1 (FP32)
+///   stage 2 (FP32 input d1):  d2 = d1 + dt/2 L d1        (= dt/2 L k1)     -> d2 (FP32)
+///   stage 3 (FP32 input d2):  d3 = 2 d1 + dt L d2        (= dt L k2),
+///                             u_new = u_p + dt/6 (2 d1 + 2 d2 + d3)  in FP64, in place
+/// Algebraically u_new = u + dt/6 (k0 + 2 k1 + 2 k2 + k3) with k_s = F(u + a_s dt k_{s-1}).
 struct EpiF32S0 {
     struct Params {
-        float* k0;
-        Layout Lf;
+        double* k0;
+        double* up;
+        Layout Lu;
+        double dt;
     };
     template <int NC> struct Pre {};
     template <int NC> static __device__ __forceinline__ Pre<NC> load(const Params&, int, int, int) { return {}; }
     template <class T, int NC>
-    static __device__ __forceinline__ void apply(const Params& p, const T (&k)[NC], const T*, int, int i, int j, int z,
-                                                 const Pre<NC>&) {
+    static __device__ __forceinline__ void apply(const Params& p, const T (&k)[NC], const T* centre, int pns, int i,
+                                                 int j, int z, const Pre<NC>&) {
+        const long long u0 = p.Lu.index(i, j, z, 0), us = p.Lu.comp_stride();
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            __stcs(p.k0 + u0 + c * us, double(k[c]));
+            __stcs(p.up + u0 + c * us, double(centre[c * pns]) + p.dt * double(k[c]));
+        }
+    }
+};
+
+/// Stage 1 of the FP32-stage form: d1 = (dt/2) L k0 from the FP64 k0, stored FP32.
+struct EpiF32S1 {
+    struct Params {
+        float* d1;
+        Layout Lf;
+        double a_dt;
+    };
+    template <int NC> struct Pre {};
+    template <int NC> static __device__ __forceinline__ Pre<NC> load(const Params&, int, int, int) { return {}; }
+    template <class T, int NC>
+    static __device__ __forceinline__ void apply(const Params& p, const T (&lk)[NC], const T*, int, int i, int j,
+                                                 int z, const Pre<NC>&) {
         const long long o0 = p.Lf.index(i, j, z, 0), cs = p.Lf.comp_stride();
 #pragma unroll
-        for (int c = 0; c < NC; ++c) p.k0[o0 + c * cs] = static_cast<float>(k[c]);
+        for (int c = 0; c < NC; ++c) p.d1[o0 + c * cs] = static_cast<float>(p.a_dt * double(lk[c]));
     }
 };
 
 template <int STAGE> struct EpiF32Lin {
     struct Params {
-        float* k_out;       // stages 1, 2
-        const float* k0;    // stages 2, 3
-        const float* k1;    // stage 3
-        const double* u_in; // stage 3: state at the start of the step
-        double* u;          // stage 3: state at the end of the step
+        float* d_out;      // stages 1, 2: d1, d2
+        const float* d1;   // stage 3
+        double* u;         // stage 3: u_p in, u_new out (in place)
         Layout Lf, Lu;
-        float a_dt;         // a_s dt
-        double dt;          // stage 3
+        float a_dt;        // dt/2 (stages 1, 2), dt (stage 3)
+        double dt;         // stage 3
     };
     template <int NC> struct Pre {
-        float k0[NC], k1[NC];
-        double u[NC];
+        float d1[NC];
+        double up[NC];
     };
     template <int NC> static __device__ __forceinline__ Pre<NC> load(const Params& p, int i, int j, int z) {
         Pre<NC> r;
-        if constexpr (STAGE >= 2) {
+        if constexpr (STAGE == 3) {
             const long long o0 = p.Lf.index(i, j, z, 0), cs = p.Lf.comp_stride();
             const long long u0 = p.Lu.index(i, j, z, 0), us = p.Lu.comp_stride();
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
-                r.k0[c] = __ldcs(p.k0 + o0 + c * cs);
-                if constexpr (STAGE == 3) {
-                    r.k1[c] = __ldcs(p.k1 + o0 + c * cs);
-                    r.u[c] = __ldcs(p.u_in + u0 + c * us);
-                }
+                r.d1[c] = __ldcs(p.d1 + o0 + c * cs);
+                r.up[c] = __ldcs(p.u + u0 + c * us);
             }
         }
         return r;
@@ -324,18 +344,18 @@ template <int STAGE> struct EpiF32Lin {
         const long long o0 = p.Lf.index(i, j, z, 0), cs = p.Lf.comp_stride();
         if constexpr (STAGE == 1) {
 #pragma unroll
-            for (int c = 0; c < NC; ++c) p.k_out[o0 + c * cs] = centre[c * pns] + p.a_dt * lk[c];
+            for (int c = 0; c < NC; ++c) p.d_out[o0 + c * cs] = p.a_dt * lk[c];
         } else if constexpr (STAGE == 2) {
 #pragma unroll
-            for (int c = 0; c < NC; ++c) p.k_out[o0 + c * cs] = pre.k0[c] + p.a_dt * lk[c];
+            for (int c = 0; c < NC; ++c) p.d_out[o0 + c * cs] = centre[c * pns] + p.a_dt * lk[c];
         } else {
             const long long u0 = p.Lu.index(i, j, z, 0), us = p.Lu.comp_stride();
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
-                const float k2 = centre[c * pns];
-                const float k3 = pre.k0[c] + p.a_dt * lk[c];
-                const double sum = double(pre.k0[c]) + 2.0 * double(pre.k1[c]) + 2.0 * double(k2) + double(k3);
-                __stcs(p.u + u0 + c * us, pre.u[c] + (p.dt / 6.0) * sum);
+                const float d1 = pre.d1[c], d2 = centre[c * pns];
+                const float d3 = 2.0f * d1 + p.a_dt * lk[c];
+                const double sum = 2.0 * double(d1) + 2.0 * double(d2) + double(d3);
+                __stcs(p.u + u0 + c * us, pre.up[c] + (p.dt / 6.0) * sum);
             }
         }
     }

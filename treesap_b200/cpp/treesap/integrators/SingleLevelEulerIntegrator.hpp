@@ -38,7 +38,11 @@ class SingleLevelEulerIntegrator : public SingleLevelIntegrator<PDEModelType> {
         using Launcher = treesap_b200::StageLauncher<Tile, RHSType, treesap_b200::EpiEuler>;
         const auto shape = Launcher::shape(L, this->sm_count(), this->tile_rows, this->z_chunks);
         const CUtensorMap& tm = this->tensor_map(state_old.data(), L, TS_F64, Launcher::box_x(), Launcher::box_y(shape));
-        if (!this->dry_run_) Launcher::launch(tm, sp, model.get_rhs(), ep, shape, this->stream());
+        if (!this->dry_run_) {
+            this->clock_begin(1);
+            Launcher::launch(tm, sp, model.get_rhs(), ep, shape, this->stream());
+            this->clock_end();
+        }
         this->launches_per_step_ = 2;
         return delta_time;
     }

@@ -66,6 +66,8 @@ struct IntegratorIface {
     virtual void* state_ptr() = 0;
     virtual Layout state_layout() const = 0;
     virtual long long launches_per_step() const = 0;
+    virtual void attach_clock(treesap::KernelClock* c) = 0;
+    virtual void set_launch_shape(int rows, int chunks) = 0;
 };
 
 /// Exposes the protected time / step counters of the front-end integrators.
@@ -106,6 +108,8 @@ template <class Integ, int NC> class Adapter final : public IntegratorIface {
     void* state_ptr() override { return integ_.state().data(); }
     Layout state_layout() const override { return integ_.state().layout(); }
     long long launches_per_step() const override { return integ_.launches_per_step(); }
+    void attach_clock(treesap::KernelClock* c) override { integ_.attach_clock(c); }
+    void set_launch_shape(int rows, int chunks) override { integ_.set_launch_shape(rows, chunks); }
 
   private:
     Exposed<Integ> integ_;

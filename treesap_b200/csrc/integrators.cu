@@ -216,6 +216,30 @@ ts_status ts_integrator_use_graph(ts_integrator* it, int enable) {
     return TS_OK;
 }
 
+ts_status ts_integrator_profile(ts_integrator* it, int nsteps, int nclasses, long long* launches, double* ms) {
+    if (!it || !it->impl || nsteps < 0 || nclasses < 1 || !launches || !ms) return TS_ERR_INVALID_ARGUMENT;
+    return guarded(it->ctx, "ts_integrator_profile", [&] {
+        treesap::KernelClock clock;
+        it->impl->attach_clock(&clock);
+        try {
+            for (int q = 0; q < nsteps; ++q) it->impl->step();
+        } catch (...) {
+            it->impl->attach_clock(nullptr);
+            throw;
+        }
+        it->impl->attach_clock(nullptr);
+        cuda_check(cudaStreamSynchronize(stream_of(it)), "cudaStreamSynchronize");
+        clock.collect(nclasses, launches, ms);
+    });
+}
+
+ts_status ts_integrator_set_launch_shape(ts_integrator* it, int rows, int chunks) {
+    if (!it || !it->impl || rows < 0 || chunks < 0) return TS_ERR_INVALID_ARGUMENT;
+    drop_graphs(it);
+    it->impl->set_launch_shape(rows, chunks);
+    return TS_OK;
+}
+
 ts_status ts_integrator_last_step_timing(ts_integrator* it, double* ms, long long* launches) {
     if (!it) return TS_ERR_INVALID_ARGUMENT;
     float f = 0.f;
