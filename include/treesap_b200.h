@@ -166,6 +166,26 @@ TS_API ts_status ts_integrator_profile(ts_integrator* it, int nsteps, int nclass
  * the default shape is chosen per launch from the SM count and the domain. */
 TS_API ts_status ts_integrator_set_launch_shape(ts_integrator* it, int rows, int chunks);
 
+/* ------------------------------------------------------------------ allocation-free stepping
+ * No counterpart in the reference. For callers that must not allocate device memory: host
+ * applications that own all device memory through their own pool or arena, and loops that
+ * cannot afford cudaMalloc / cudaFree because those may synchronise the device and stall the
+ * caller's other streams. Advances `state` (a caller-owned device buffer in the layout of
+ * ts_field_layout_make(n, 2, 2, TS_F64), ghost cells included) by nsteps RK4 steps with the
+ * same fused stage kernels and ghost fills as ts_integrator_step, on `stream` (a
+ * cudaStream_t, 0 = the legacy default stream), and waits for it. Supported: TS_MODEL_WAVE,
+ * ngrow 2, optional Kreiss-Oliger, periodic / Dirichlet / NoOp boundaries, TS_RK4 in FP64;
+ * anything else returns TS_ERR_UNSUPPORTED. Simulation time restarts at 0 on every call (the
+ * supported models do not depend on time).
+ * Scratch: the three RK4 stage registers and a device error word live in one static device
+ * array of TS_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until exit; a
+ * domain whose three padded fields do not fit (about 100^3 cells) returns
+ * TS_ERR_INVALID_ARGUMENT before any work. The first call on a device looks up the array's
+ * device address; make that first call before any stream capture. All calls share the array
+ * (each call clears it first), so calls whose GPU work overlaps, on any streams, race. */
+#define TS_NOALLOC_SCRATCH_BYTES (48ull * 1024ull * 1024ull)
+TS_API ts_status ts_wave_rk4_steps_noalloc(const ts_wave_desc* desc, double* state, int nsteps, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
