@@ -62,19 +62,14 @@ struct KernelClock {
 namespace detail {
 /// Tile shape of the fused stage kernel for a value type, ghost width and component count:
 /// 32-wide rows (one warp each), up to 7 rows plus the producer warp (256 threads, two CTAs
-/// per SM within the register file), and the deepest plane ring (prefetch distance P <= 4)
-/// that leaves room for two CTAs per SM; fewer rows and one CTA per SM for many components.
+/// per SM within the register file) with up to P = 4 planes of prefetch (fewer when the ring,
+/// including two FP64 centre-operand boxes per slot, would not leave room for two CTAs per
+/// SM); fewer rows and one CTA per SM for many components.
 template <typename T, int G, int NC> struct DefaultTile {
     template <int TY, int P, int MINB = 2> using C = treesap_b200::TileCfg<32, TY, G, NC, T, P, MINB>;
-    static constexpr int kTwoPerSM = 113 * 1024, kOnePerSM = 220 * 1024;
     using type = std::conditional_t<
-        (C<7, 4>::SMEM <= kTwoPerSM), C<7, 4>,
-        std::conditional_t<
-            (C<7, 3>::SMEM <= kTwoPerSM), C<7, 3>,
-            std::conditional_t<(C<7, 2>::SMEM <= kTwoPerSM), C<7, 2>,
-                               std::conditional_t<(C<3, 2>::SMEM <= kTwoPerSM), C<3, 2>,
-                                                  std::conditional_t<(C<3, 1, 1>::SMEM <= kOnePerSM), C<3, 1, 1>,
-                                                                     C<1, 1, 1>>>>>>;
+        C<7, 4>::fits, C<7, 4>,
+        std::conditional_t<C<3, 2>::fits, C<3, 2>, std::conditional_t<C<3, 2, 1>::fits, C<3, 2, 1>, C<1, 1, 1>>>>;
 };
 } // namespace detail
 
@@ -221,6 +216,16 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
 
     const CUtensorMap& tensor_map(const void* base, const treesap_b200::Layout& L, int dtype, int box_x, int box_y) {
         return tmaps.get(base, L, dtype, box_x, box_y);
+    }
+
+    /// TMA descriptors of a stage launch's centre-operand fields (cached like tensor_map).
+    template <class Launcher, class Params>
+    treesap_b200::CentreMaps centre_maps(const Params& ep, const treesap_b200::LaunchShape& shape) {
+        return Launcher::centre_maps(
+            [this](const void* b, const treesap_b200::Layout& L, int dtype, int bx, int by) -> const CUtensorMap& {
+                return tmaps.get(b, L, dtype, bx, by);
+            },
+            ep, shape);
     }
 
     static const int* extent_of(const amrex::Geometry& g, int* n) {

@@ -40,11 +40,11 @@ inline ts_context* default_context() {
     return ctx;
 }
 
-/// Cache of TMA descriptors, keyed by (device pointer, box).
+/// Cache of TMA descriptors, keyed by (device pointer, box, extents, element type).
 class TensorMapCache {
   public:
     const CUtensorMap& get(const void* base, const Layout& L, int dtype, int box_x, int box_y) {
-        auto key = std::make_tuple(base, box_x, box_y, L.px, L.py, L.pz);
+        auto key = std::make_tuple(base, box_x, box_y, L.px, L.py, L.pz, dtype);
         auto it = maps_.find(key);
         if (it != maps_.end()) return it->second;
         CUtensorMap m;
@@ -55,7 +55,7 @@ class TensorMapCache {
     void clear() { maps_.clear(); }
 
   private:
-    std::map<std::tuple<const void*, int, int, long long, long long, long long>, CUtensorMap> maps_;
+    std::map<std::tuple<const void*, int, int, long long, long long, long long, int>, CUtensorMap> maps_;
 };
 
 } // namespace treesap_b200

@@ -9,26 +9,31 @@
 //   * the producer warp's elected lane copies the plane's tile plus its ghost halo, all
 //     components, with one TMA load (cp.async.bulk.tensor.4d, no multicast; box
 //     (TX+2*XH) x (TY+2G) x 1 x NC, zero fill outside the array) into a ring of R shared-memory
-//     slots. Slot s has a `full` mbarrier (TMA transaction count) and an `empty` mbarrier
-//     (one arrival per consumer warp); the producer refills a slot once every consumer warp
-//     has released it, running up to R - G - 1 planes ahead of the computation.
+//     slots. When the plane is also a stencil centre plane of this CTA, the same slot receives
+//     the epilogue's centre operands (the stage registers it reads at the centre cells, e.g.
+//     the RK4 accumulator and initial state): one more TMA box (TX x TY x 1 x NC) per operand
+//     field, completing on the same barrier. Slot s has a `full` mbarrier (TMA transaction
+//     count) and an `empty` mbarrier (one arrival per consumer warp); the producer refills a
+//     slot once every consumer warp has released it, running up to R - G - 1 planes ahead of
+//     the queue and R - 1 planes ahead of the centre computation.
 //   * each consumer thread keeps its column's values at z-G .. z+G in a register queue,
 //     shifted once per plane and fed from the newest plane.
 //   * the user's RHS functor is called once per component, in component order, on an Array4
 //     whose StencilView resolves every access at compile time: same-z offsets to the
 //     shared-memory plane, same-column offsets to the register queue, anything else
 //     (mixed x-z / y-z derivatives) to global memory.
-//   * an epilogue policy combines the stage values with centre operands loaded one plane
-//     ahead (register double buffer) and stores the results with coalesced stores.
+//   * an epilogue policy combines the stage values with the centre operands from shared memory
+//     and stores the results with coalesced stores.
 //
 // No CTA-wide barrier in the plane loop: warps proceed independently, bounded only by the
 // ring. Every wait is bounded (ptx.cuh); on a timeout the kernel records an error bit, lets
 // in-flight copies land and returns.
 //
 // Ring bookkeeping (per chunk, plane index it = 0 .. NP-1, z = z0 - G + it): plane it feeds the
-// queue at iteration it and, when z0 <= z < z1, the x-y stencil taps at iteration it + G. After
-// iteration it a consumer warp has released planes [0, released(it)):
-//   released(it) = it + 1 (it < G),  G (G <= it < 2G),  it - G + 1 (it >= 2G),  NP (last).
+// queue at iteration it and, when z0 <= z < z1, the x-y stencil taps and the centre operands at
+// iteration it + G. Each consumer warp releases plane p after iteration p (p < G) or p + G
+// (p >= G), one plane per iteration; the producer refills a slot with plane q once plane q - R
+// is released (R >= G + 2, so the newest plane never waits on a plane still in use).
 #pragma once
 
 #include <AMReX.H>
@@ -43,22 +48,49 @@
 
 namespace treesap_b200 {
 
+constexpr int align128(int b) { return (b + 127) / 128 * 128; }
+
 template <int TX_, int TYMAX_, int G_, int NC_, typename T_, int P_ = 2, int MINB_ = 2> struct TileCfg {
     using T = T_;
     static constexpr int TX = TX_, TYMAX = TYMAX_, G = G_, NC = NC_, P = P_;
-    static constexpr int MIN_BLOCKS = MINB_; // resident CTAs per SM the register budget is sized for
+    static constexpr int MIN_BLOCKS = MINB_; // resident CTAs per SM the register and smem budgets are sized for
     static constexpr int A = 16 / int(sizeof(T));   // elements per 16 bytes
     static constexpr int XH = (G + A - 1) / A * A;  // x halo width in shared memory (16-byte aligned)
     static constexpr int BX = TX + 2 * XH;
     static constexpr int BYMAX = TYMAX + 2 * G;
-    static constexpr int PLANE_MAX = NC * BYMAX * BX; // elements per slot (at TYMAX)
-    static constexpr int R = G + 1 + P;               // ring slots
-    static constexpr int THREADS = TX * TYMAX + 32;   // consumer warps + one producer warp
-    static constexpr int SLOT_BYTES = (PLANE_MAX * int(sizeof(T)) + 127) / 128 * 128;
-    static constexpr int SMEM = R * SLOT_BYTES + 16 * R;
+    static constexpr int PLANE_MAX = NC * BYMAX * BX;  // stencil elements per slot (at TYMAX)
+    static constexpr int THREADS = TX * TYMAX + 32;    // consumer warps + one producer warp
+    static constexpr int STENCIL_BYTES = align128(PLANE_MAX * int(sizeof(T)));
+    static constexpr int CBOX = NC * TYMAX * TX;       // elements of one centre-operand box
+    /// Dynamic shared memory per CTA when MIN_BLOCKS CTAs share an SM (228 KB per SM with 1 KB
+    /// reserved per CTA; at most 227 KB for one CTA).
+    static constexpr int SMEM_BUDGET = MINB_ == 1 ? 232448 : 233472 / MINB_ - 1024;
+    /// Ring slots of a given slot size: G + 1 + P, or fewer when the budget is smaller.
+    static constexpr int ring_slots(int slot_bytes) {
+        const int r = SMEM_BUDGET / (slot_bytes + 16);
+        return r < G + 1 + P ? r : G + 1 + P;
+    }
+    /// Usable when even two FP64 centre-operand fields leave one plane of prefetch.
+    static constexpr bool fits = ring_slots(STENCIL_BYTES + 2 * align128(CBOX * 8)) >= G + 2;
     static_assert(TX == 32, "one warp per tile row");
     static_assert(BX <= 256 && BYMAX <= 256 && NC <= 256, "TMA box dimensions are limited to 256");
     static_assert(THREADS <= 1024, "too many threads");
+};
+
+/// Shared-memory ring of one (tile configuration, epilogue) pair. A slot holds the stencil
+/// plane ([comp][y][x], TY + 2G rows of BX) followed by the epilogue's centre-operand boxes
+/// ([comp][y][x], TY rows of TX), each 128-byte aligned.
+template <class Cfg, class Epi> struct Ring {
+    using C0 = typename Epi::C0;
+    using C1 = typename Epi::C1;
+    static constexpr int NCEN = Epi::kCentre;
+    static_assert(NCEN >= 0 && NCEN <= 2, "at most two centre-operand fields");
+    static constexpr int C0_OFF = Cfg::STENCIL_BYTES;
+    static constexpr int C1_OFF = C0_OFF + (NCEN > 0 ? align128(Cfg::CBOX * int(sizeof(C0))) : 0);
+    static constexpr int SLOT = C1_OFF + (NCEN > 1 ? align128(Cfg::CBOX * int(sizeof(C1))) : 0);
+    static constexpr int R = Cfg::ring_slots(SLOT);
+    static constexpr int SMEM = R * SLOT + 16 * R;
+    static_assert(R >= Cfg::G + 2, "shared-memory ring too small for this tile configuration");
 };
 
 /// Launch-invariant stage inputs.
@@ -73,22 +105,46 @@ template <typename T> struct StageParams {
     int* err;                 // device error word
 };
 
+/// TMA descriptors of the centre-operand fields (box TX x ty x 1 x NC) and the storage
+/// coordinates of cell (0, 0, 0) in each (x = xoff, y = z = ngrow).
+struct alignas(64) CentreMaps {
+    CUtensorMap map[2];
+    int x[2], y[2], z[2];
+};
+
+/// What an epilogue reads at its centre cell: component c of operand field k is ck[c * cps].
+template <class C0, class C1> struct CentreOps {
+    const C0* c0;
+    const C1* c1;
+    int cps;
+};
+
+/// Host-side description of one centre-operand field.
+struct CentreSrc {
+    const void* base;
+    Layout L;
+    int dtype; // ts_dtype
+};
+
 template <class Cfg, class RHS, class Epi>
 __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
-    stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageParams<typename Cfg::T> sp, const RHS rhs,
-                 const typename Epi::Params ep) {
+    stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CentreMaps cmaps,
+                 const StageParams<typename Cfg::T> sp, const RHS rhs, const typename Epi::Params ep) {
     using T = typename Cfg::T;
-    constexpr int G = Cfg::G, NC = Cfg::NC, TX = Cfg::TX, BX = Cfg::BX, R = Cfg::R, XH = Cfg::XH;
-    constexpr int SLOT = Cfg::SLOT_BYTES / int(sizeof(T));
+    using RingT = Ring<Cfg, Epi>;
+    using C0 = typename RingT::C0;
+    using C1 = typename RingT::C1;
+    constexpr int G = Cfg::G, NC = Cfg::NC, TX = Cfg::TX, BX = Cfg::BX, XH = Cfg::XH;
+    constexpr int R = RingT::R, SLOT = RingT::SLOT, NCEN = RingT::NCEN;
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    T* ring = reinterpret_cast<T*>(smem_raw);
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + R * Cfg::SLOT_BYTES);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + R * SLOT);
     uint64_t* empty = full + R;
 
     const int TY = sp.ty;
     const int BY = TY + 2 * G;
-    const int PNS = BY * BX; // component stride inside a slot
+    const int PNS = BY * BX; // component stride of the stencil plane inside a slot
+    const int CPS = TY * TX; // component stride of a centre-operand box inside a slot
     const int ntiles = sp.ntx * sp.nty;
     const int tile = blockIdx.x % ntiles;
     const int z0 = (blockIdx.x / ntiles) * sp.zchunk;
@@ -111,14 +167,37 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
         // ---------------------------------------------------------------- producer warp
         if (lane == 0) {
             ptx::prefetch_tensor_map(&tmap);
+            if constexpr (NCEN > 0) ptx::prefetch_tensor_map(&cmaps.map[0]);
+            if constexpr (NCEN > 1) ptx::prefetch_tensor_map(&cmaps.map[1]);
             const uint32_t bytes = uint32_t(NC * BY * BX * int(sizeof(T)));
-            int q = 0;
+            uint32_t cbytes = 0;
+            if constexpr (NCEN > 0) cbytes += uint32_t(NC * TY * TX * int(sizeof(C0)));
+            if constexpr (NCEN > 1) cbytes += uint32_t(NC * TY * TX * int(sizeof(C1)));
+            // slot s of plane q; before refilling it, wait for completion q / R of empty[s]
+            // (parity (q / R - 1) & 1), i.e. the release of plane q - R
+            int q = 0, s = 0;
+            uint32_t ph = 1;
             for (; q < NP; ++q) {
-                const int s = q % R;
-                if (q >= R && !ptx::mbar_wait(&empty[s], uint32_t(((q / R) - 1) & 1), sp.err)) break;
-                ptx::mbar_arrive_expect_tx(&full[s], bytes);
-                // storage coordinates: x = x0 - XH + xoff (= x0), y = y0 - G + g (= y0), z = z0 - G + q + g
-                ptx::tma_load_4d(ring + s * SLOT, &tmap, x0, y0, z0 + q, 0, &full[s]);
+                if (q >= R && !ptx::mbar_wait(&empty[s], ph, sp.err)) break;
+                const int zq = z0 - G + q;
+                const bool centre = NCEN > 0 && zq >= z0 && zq < z1;
+                unsigned char* slot = smem_raw + s * SLOT;
+                ptx::mbar_arrive_expect_tx(&full[s], bytes + (centre ? cbytes : 0u));
+                // storage coordinates: x = x0 - XH + xoff (= x0), y = y0 - G + g (= y0), z = zq + g
+                ptx::tma_load_4d(slot, &tmap, x0, y0, z0 + q, 0, &full[s]);
+                if constexpr (NCEN > 0) {
+                    if (centre) {
+                        ptx::tma_load_4d(slot + RingT::C0_OFF, &cmaps.map[0], x0 + cmaps.x[0], y0 + cmaps.y[0],
+                                         zq + cmaps.z[0], 0, &full[s]);
+                        if constexpr (NCEN > 1)
+                            ptx::tma_load_4d(slot + RingT::C1_OFF, &cmaps.map[1], x0 + cmaps.x[1],
+                                             y0 + cmaps.y[1], zq + cmaps.z[1], 0, &full[s]);
+                    }
+                }
+                if (++s == R) {
+                    s = 0;
+                    ph ^= 1u;
+                }
             }
             if (q < NP) {
                 // a consumer warp stopped releasing slots: let the copies in flight land
@@ -143,33 +222,36 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
     const int tx = lane, ty = warp;
     const int i = x0 + tx, j = y0 + ty;
     const bool active = (i < L.n[0]) && (j < L.n[1]);
-    const int coff = (ty + G) * BX + (tx + XH); // this thread's centre inside a slot
+    const int coff = (ty + G) * BX + (tx + XH); // this thread's centre inside the stencil plane
+    const int cc = ty * TX + tx;                // ... inside a centre-operand box
 
     T q[(2 * G + 1) * NC]; // register queue: q[(dk + G) * NC + c]
 #pragma unroll
     for (int e = 0; e < (2 * G + 1) * NC; ++e) q[e] = T(0);
 
-    using Pre = typename Epi::template Pre<NC>;
-    Pre pre{};
-    if (active) pre = Epi::template load<NC>(epl, i, j, z0);
     const T* in_col = sp.in + L.index(i, j, 0, 0); // global fallback: this column at z = 0
     const long long plane = L.px * L.py;
 
-    int released = 0;
+    // s: slot of plane it (full-barrier parity ph); sc: slot of plane it - G, the stencil centre
+    // plane of iteration it. Plane p is released after iteration p (p < G: halo planes below the
+    // chunk) or p + G (its use as a centre plane); the last G planes need no release, since no
+    // copy waits for their slots.
+    int s = 0, sc = R - G;
+    uint32_t ph = 0;
     for (int it = 0; it < NP; ++it) {
-        const int s = it % R;
-        if (!ptx::mbar_wait(&full[s], uint32_t((it / R) & 1), sp.err)) break;
-        const T* slot = ring + s * SLOT;
+        if (!ptx::mbar_wait(&full[s], ph, sp.err)) break;
+        const T* newest = reinterpret_cast<const T*>(smem_raw + s * SLOT);
 #pragma unroll
         for (int e = 0; e < 2 * G * NC; ++e) q[e] = q[e + NC];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) q[2 * G * NC + c] = slot[c * PNS + coff];
+        for (int c = 0; c < NC; ++c) q[2 * G * NC + c] = newest[c * PNS + coff];
 
         if (it >= 2 * G && active) {
             const int z = z0 - 2 * G + it;
-            Pre pre_next{};
-            if (z + 1 < z1) pre_next = Epi::template load<NC>(epl, i, j, z + 1);
-            const T* ctr = ring + ((it - G) % R) * SLOT + coff;
+            const unsigned char* cslot = smem_raw + sc * SLOT;
+            const T* ctr = reinterpret_cast<const T*>(cslot) + coff;
+            const CentreOps<C0, C1> co{reinterpret_cast<const C0*>(cslot + RingT::C0_OFF) + cc,
+                                       reinterpret_cast<const C1*>(cslot + RingT::C1_OFF) + cc, CPS};
             amrex::StencilView<T> view{ctr, q, in_col + z * plane, L.px, plane, L.comp_stride(), i, j, z, BX, PNS,
                                        G, NC};
             amrex::Array4<const T> arr = make_array4<const T>(sp.in, L);
@@ -180,29 +262,44 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
             treesap::static_for<NC>([&]<int c>() {
                 kv[c] = static_cast<T>(f.template operator()<c>(idx, time, arr, geom, ws));
             });
-            Epi::template apply<T, NC>(epl, kv, ctr, PNS, i, j, z, pre);
-            pre = pre_next;
+            Epi::template apply<T, NC>(epl, kv, ctr, PNS, i, j, z, co);
         }
-        int rel = (it < G) ? it + 1 : (it < 2 * G ? G : it - G + 1);
-        if (it == NP - 1) rel = NP;
         __syncwarp();
-        if (lane == 0)
-            for (int r = released; r < rel; ++r) ptx::mbar_arrive(&empty[r % R]);
-        released = rel;
+        if (lane == 0) {
+            if (it < G)
+                ptx::mbar_arrive(&empty[s]);
+            else if (it >= 2 * G)
+                ptx::mbar_arrive(&empty[sc]);
+        }
+        if (++s == R) {
+            s = 0;
+            ph ^= 1u;
+        }
+        if (++sc == R) sc = 0;
     }
 }
 
 // ------------------------------------------------------------------ epilogues
-// Each policy: struct Params; struct Pre (centre operands loaded one plane ahead);
-// static Pre load(params, i, j, z); template <T, NC> static void apply(params, k[NC], centre,
-// pns, i, j, z, pre) where `centre` points at component 0 of the stencil input's centre in
-// shared memory.
+// Each policy: struct Params; kCentre (0..2) centre-operand fields of element types C0, C1,
+// described on the host by centre_src(params, k); and
+//   template <T, NC, CO> static void apply(params, k[NC], centre, pns, i, j, z, co)
+// where `centre` points at component 0 of the stencil input's centre in shared memory and
+// co.c0 / co.c1 at component 0 of the centre operands (component stride co.cps).
+
+/// Epilogue without centre operands.
+struct NoCentre {
+    static constexpr int kCentre = 0;
+    using C0 = char;
+    using C1 = char;
+    static CentreSrc centre_src(...) { return {}; }
+};
 
 /// FP64 plain RK4 stage s with the reference's register scheme
 /// (integrators/SingleLevelRK4Integrator.hpp:139-155):
 ///   s = 0:   acc = init + b k,  arg_next = init + a_next k   (the stencil input is init)
 ///   s = 1,2: acc += b k,        arg_next = init + a_next k
 ///   s = 3:   acc += b k
+/// Centre operands (s > 0): acc (C0) and, for s < 3, init (C1).
 template <int STAGE> struct EpiRK4 {
     struct Params {
         double* acc;
@@ -211,25 +308,15 @@ template <int STAGE> struct EpiRK4 {
         Layout L;
         double b, a_next;
     };
-    template <int NC> struct Pre {
-        double acc[NC];
-        double init[NC];
-    };
-    template <int NC> static __device__ __forceinline__ Pre<NC> load(const Params& p, int i, int j, int z) {
-        Pre<NC> r;
-        if constexpr (STAGE > 0) {
-            const long long o0 = p.L.index(i, j, z, 0), cs = p.L.comp_stride();
-#pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                r.acc[c] = __ldcs(p.acc + o0 + c * cs);
-                if constexpr (STAGE < 3) r.init[c] = __ldg(p.init + o0 + c * cs);
-            }
-        }
-        return r;
+    static constexpr int kCentre = STAGE == 0 ? 0 : (STAGE < 3 ? 2 : 1);
+    using C0 = double;
+    using C1 = double;
+    static CentreSrc centre_src(const Params& p, int k) {
+        return k == 0 ? CentreSrc{p.acc, p.L, TS_F64} : CentreSrc{p.init, p.L, TS_F64};
     }
-    template <class T, int NC>
+    template <class T, int NC, class CO>
     static __device__ __forceinline__ void apply(const Params& p, const T (&k)[NC], const T* centre, int pns, int i,
-                                                 int j, int z, const Pre<NC>& pre) {
+                                                 int j, int z, const CO& co) {
         const long long o0 = p.L.index(i, j, z, 0), cs = p.L.comp_stride();
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
@@ -239,25 +326,23 @@ template <int STAGE> struct EpiRK4 {
                 __stcs(p.acc + o, u0 + p.b * k[c]);
                 __stcs(p.arg_next + o, u0 + p.a_next * k[c]);
             } else {
-                if constexpr (STAGE < 3) __stcs(p.arg_next + o, pre.init[c] + p.a_next * k[c]);
-                __stcs(p.acc + o, pre.acc[c] + p.b * k[c]);
+                if constexpr (STAGE < 3) __stcs(p.arg_next + o, co.c1[c * co.cps] + p.a_next * k[c]);
+                __stcs(p.acc + o, co.c0[c * co.cps] + p.b * k[c]);
             }
         }
     }
 };
 
 /// Forward Euler (integrators/SingleLevelEulerIntegrator.hpp:77-84): new = old + dt k.
-struct EpiEuler {
+struct EpiEuler : NoCentre {
     struct Params {
         double* out;
         Layout L;
         double dt;
     };
-    template <int NC> struct Pre {};
-    template <int NC> static __device__ __forceinline__ Pre<NC> load(const Params&, int, int, int) { return {}; }
-    template <class T, int NC>
+    template <class T, int NC, class CO>
     static __device__ __forceinline__ void apply(const Params& p, const T (&k)[NC], const T* centre, int pns, int i,
-                                                 int j, int z, const Pre<NC>&) {
+                                                 int j, int z, const CO&) {
         const long long o0 = p.L.index(i, j, z, 0), cs = p.L.comp_stride();
 #pragma unroll
         for (int c = 0; c < NC; ++c) __stcs(p.out + o0 + c * cs, centre[c * pns] + p.dt * k[c]);
@@ -273,18 +358,16 @@ struct EpiEuler {
 ///   stage 3 (FP32 input d2):  d3 = 2 d1 + dt L d2        (= dt L k2),
 ///                             u_new = u_p + dt/6 (2 d1 + 2 d2 + d3)  in FP64, in place
 /// Algebraically u_new = u + dt/6 (k0 + 2 k1 + 2 k2 + k3) with k_s = F(u + a_s dt k_{s-1}).
-struct EpiF32S0 {
+struct EpiF32S0 : NoCentre {
     struct Params {
         double* k0;
         double* up;
         Layout Lu;
         double dt;
     };
-    template <int NC> struct Pre {};
-    template <int NC> static __device__ __forceinline__ Pre<NC> load(const Params&, int, int, int) { return {}; }
-    template <class T, int NC>
+    template <class T, int NC, class CO>
     static __device__ __forceinline__ void apply(const Params& p, const T (&k)[NC], const T* centre, int pns, int i,
-                                                 int j, int z, const Pre<NC>&) {
+                                                 int j, int z, const CO&) {
         const long long u0 = p.Lu.index(i, j, z, 0), us = p.Lu.comp_stride();
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
@@ -295,23 +378,23 @@ struct EpiF32S0 {
 };
 
 /// Stage 1 of the FP32-stage form: d1 = (dt/2) L k0 from the FP64 k0, stored FP32.
-struct EpiF32S1 {
+struct EpiF32S1 : NoCentre {
     struct Params {
         float* d1;
         Layout Lf;
         double a_dt;
     };
-    template <int NC> struct Pre {};
-    template <int NC> static __device__ __forceinline__ Pre<NC> load(const Params&, int, int, int) { return {}; }
-    template <class T, int NC>
+    template <class T, int NC, class CO>
     static __device__ __forceinline__ void apply(const Params& p, const T (&lk)[NC], const T*, int, int i, int j,
-                                                 int z, const Pre<NC>&) {
+                                                 int z, const CO&) {
         const long long o0 = p.Lf.index(i, j, z, 0), cs = p.Lf.comp_stride();
 #pragma unroll
         for (int c = 0; c < NC; ++c) p.d1[o0 + c * cs] = static_cast<float>(p.a_dt * double(lk[c]));
     }
 };
 
+/// Stages 2 and 3 of the FP32-stage form. Centre operands of stage 3: d1 (C0, FP32) and
+/// u_p (C1, FP64).
 template <int STAGE> struct EpiF32Lin {
     struct Params {
         float* d_out;      // stages 1, 2: d1, d2
@@ -321,26 +404,15 @@ template <int STAGE> struct EpiF32Lin {
         float a_dt;        // dt/2 (stages 1, 2), dt (stage 3)
         double dt;         // stage 3
     };
-    template <int NC> struct Pre {
-        float d1[NC];
-        double up[NC];
-    };
-    template <int NC> static __device__ __forceinline__ Pre<NC> load(const Params& p, int i, int j, int z) {
-        Pre<NC> r;
-        if constexpr (STAGE == 3) {
-            const long long o0 = p.Lf.index(i, j, z, 0), cs = p.Lf.comp_stride();
-            const long long u0 = p.Lu.index(i, j, z, 0), us = p.Lu.comp_stride();
-#pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                r.d1[c] = __ldcs(p.d1 + o0 + c * cs);
-                r.up[c] = __ldcs(p.u + u0 + c * us);
-            }
-        }
-        return r;
+    static constexpr int kCentre = STAGE == 3 ? 2 : 0;
+    using C0 = float;
+    using C1 = double;
+    static CentreSrc centre_src(const Params& p, int k) {
+        return k == 0 ? CentreSrc{p.d1, p.Lf, TS_F32} : CentreSrc{p.u, p.Lu, TS_F64};
     }
-    template <class T, int NC>
+    template <class T, int NC, class CO>
     static __device__ __forceinline__ void apply(const Params& p, const T (&lk)[NC], const T* centre, int pns, int i,
-                                                 int j, int z, const Pre<NC>& pre) {
+                                                 int j, int z, const CO& co) {
         const long long o0 = p.Lf.index(i, j, z, 0), cs = p.Lf.comp_stride();
         if constexpr (STAGE == 1) {
 #pragma unroll
@@ -352,10 +424,10 @@ template <int STAGE> struct EpiF32Lin {
             const long long u0 = p.Lu.index(i, j, z, 0), us = p.Lu.comp_stride();
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
-                const float d1 = pre.d1[c], d2 = centre[c * pns];
+                const float d1 = co.c0[c * co.cps], d2 = centre[c * pns];
                 const float d3 = 2.0f * d1 + p.a_dt * lk[c];
                 const double sum = 2.0 * double(d1) + 2.0 * double(d2) + double(d3);
-                __stcs(p.u + u0 + c * us, pre.up[c] + (p.dt / 6.0) * sum);
+                __stcs(p.u + u0 + c * us, co.c1[c * co.cps] + (p.dt / 6.0) * sum);
             }
         }
     }
@@ -408,6 +480,7 @@ template <class Cfg> int choose_ty(const Layout& L, int slots) {
 }
 
 template <class Cfg, class RHS, class Epi> struct StageLauncher {
+    using RingT = Ring<Cfg, Epi>;
     static auto kernel() { return &stage_kernel<Cfg, RHS, Epi>; }
     /// Resident CTAs per SM for this instantiation (sets the dynamic shared-memory limit once per device).
     static int occupancy() {
@@ -416,10 +489,10 @@ template <class Cfg, class RHS, class Epi> struct StageLauncher {
         cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
         if (dev < 0 || dev >= 64) dev = 0;
         if (occ[dev] == 0) {
-            cuda_check(cudaFuncSetAttribute(kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM),
+            cuda_check(cudaFuncSetAttribute(kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, RingT::SMEM),
                        "cudaFuncSetAttribute(smem)");
             int nb = 0;
-            cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel(), Cfg::THREADS, Cfg::SMEM),
+            cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel(), Cfg::THREADS, RingT::SMEM),
                        "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
             occ[dev] = nb > 0 ? nb : 1;
         }
@@ -431,17 +504,31 @@ template <class Cfg, class RHS, class Epi> struct StageLauncher {
         if (ty <= 0 || ty > Cfg::TYMAX) ty = choose_ty<Cfg>(L, slots);
         return make_shape<Cfg>(L, slots, ty, nchunks);
     }
-    /// The TMA box of a launch shape: (TX + 2 XH) x (ty + 2G).
+    /// The TMA box of the stencil input for a launch shape: (TX + 2 XH) x (ty + 2G).
     static int box_x() { return Cfg::BX; }
     static int box_y(const LaunchShape& s) { return s.ty + 2 * Cfg::G; }
-    static void launch(const CUtensorMap& tmap, StageParams<typename Cfg::T> sp, const RHS& rhs,
-                       const typename Epi::Params& ep, const LaunchShape& s, cudaStream_t stream) {
+    /// Centre-operand descriptors (box TX x ty) from `map(base, layout, dtype, box_x, box_y)`,
+    /// which returns a const CUtensorMap&.
+    template <class MapFn>
+    static CentreMaps centre_maps(MapFn&& map, const typename Epi::Params& ep, const LaunchShape& s) {
+        CentreMaps cm{};
+        for (int k = 0; k < Epi::kCentre; ++k) {
+            const CentreSrc src = Epi::centre_src(ep, k);
+            cm.map[k] = map(src.base, src.L, src.dtype, Cfg::TX, s.ty);
+            cm.x[k] = src.L.xoff;
+            cm.y[k] = src.L.g;
+            cm.z[k] = src.L.g;
+        }
+        return cm;
+    }
+    static void launch(const CUtensorMap& tmap, const CentreMaps& cmaps, StageParams<typename Cfg::T> sp,
+                       const RHS& rhs, const typename Epi::Params& ep, const LaunchShape& s, cudaStream_t stream) {
         sp.ntx = s.ntx;
         sp.nty = s.nty;
         sp.ty = s.ty;
         sp.zchunk = s.zchunk;
         const int threads = 32 * s.ty + 32;
-        stage_kernel<Cfg, RHS, Epi><<<s.grid, threads, Cfg::SMEM, stream>>>(tmap, sp, rhs, ep);
+        stage_kernel<Cfg, RHS, Epi><<<s.grid, threads, RingT::SMEM, stream>>>(tmap, cmaps, sp, rhs, ep);
         cuda_check(cudaGetLastError(), "stage_kernel launch");
     }
 };

@@ -40,7 +40,8 @@ class SingleLevelEulerIntegrator : public SingleLevelIntegrator<PDEModelType> {
         const CUtensorMap& tm = this->tensor_map(state_old.data(), L, TS_F64, Launcher::box_x(), Launcher::box_y(shape));
         if (!this->dry_run_) {
             this->clock_begin(1);
-            Launcher::launch(tm, sp, model.get_rhs(), ep, shape, this->stream());
+            Launcher::launch(tm, this->template centre_maps<Launcher>(ep, shape), sp, model.get_rhs(), ep, shape,
+                             this->stream());
             this->clock_end();
         }
         this->launches_per_step_ = 2;

@@ -73,8 +73,9 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
             const auto shape = Launcher::shape(Lu, this->sm_count(), this->tile_rows, this->z_chunks);
             const CUtensorMap& tm =
                 this->tensor_map(state_old.data(), Lu, TS_F64, Launcher::box_x(), Launcher::box_y(shape));
+            const CentreMaps cm = this->template centre_maps<Launcher>(ep, shape);
             this->clock_begin(1);
-            Launcher::launch(tm, sp, model.get_rhs(), ep, shape, this->stream());
+            Launcher::launch(tm, cm, sp, model.get_rhs(), ep, shape, this->stream());
             this->clock_end();
         }
         fill_increment(k0);
@@ -90,8 +91,9 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
             using Launcher = StageLauncher<Tile64, LinearRHS, EpiF32S1>;
             const auto shape = Launcher::shape(Lu, this->sm_count(), this->tile_rows, this->z_chunks);
             const CUtensorMap& tm = this->tensor_map(k0.data(), Lu, TS_F64, Launcher::box_x(), Launcher::box_y(shape));
+            const CentreMaps cm = this->template centre_maps<Launcher>(ep, shape);
             this->clock_begin(2);
-            Launcher::launch(tm, sp, lin, ep, shape, this->stream());
+            Launcher::launch(tm, cm, sp, lin, ep, shape, this->stream());
             this->clock_end();
         }
         fill_increment(d1);
@@ -122,8 +124,9 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
         using Launcher = StageLauncher<Tile32, LinearRHS, EpiF32Lin<S>>;
         const auto shape = Launcher::shape(Lf, this->sm_count(), this->tile_rows, this->z_chunks);
         const CUtensorMap& tm = this->tensor_map(in.data(), Lf, TS_F32, Launcher::box_x(), Launcher::box_y(shape));
+        const CentreMaps cm = this->template centre_maps<Launcher>(ep, shape);
         this->clock_begin(1 + S);
-        Launcher::launch(tm, sp, lin, ep, shape, this->stream());
+        Launcher::launch(tm, cm, sp, lin, ep, shape, this->stream());
         this->clock_end();
     }
 

@@ -28,7 +28,14 @@ struct ABLDecorator {
     static constexpr int ncomp = RHSType::ncomp;
     static constexpr int ngrow = RHSType::ngrow;
     static constexpr bool is_affine_autonomous = is_affine_autonomous_v<RHSType>;
-    using Workspace = typename RHSType::Workspace;
+    /// The wrapped model's workspace plus this cell's damping strength, computed by the first
+    /// component evaluated in the cell and reused by the others (the integrators create one
+    /// workspace per cell).
+    struct Workspace {
+        typename RHSType::Workspace inner{};
+        bool have_sigma = false;
+        amrex::Real sigma_value = 0.0;
+    };
 
     struct ABLData {
         ABLData(amrex::GpuArray<amrex::Real, ncomp> target_values_, int thickness_, amrex::Real max_strength_,
@@ -50,17 +57,23 @@ struct ABLDecorator {
     AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE T operator()(const amrex::IntVect idx, amrex::Real time,
                                                           const amrex::Array4<const T>& arr,
                                                           const amrex::GeometryData& geom, Workspace& ws) const {
-        return T(rhs.template operator()<comp>(idx, time, arr, geom, ws)) -
-               T(sigma(idx)) * (arr(idx, comp) - T(data.target_values[comp]));
+        if (!ws.have_sigma) {
+            ws.sigma_value = sigma(idx);
+            ws.have_sigma = true;
+        }
+        return T(rhs.template operator()<comp>(idx, time, arr, geom, ws.inner)) -
+               T(ws.sigma_value) * (arr(idx, comp) - T(data.target_values[comp]));
     }
 
+    /// 0 inside the bulk (where the clamped distance vanishes), else the profile of the
+    /// Euclidean index distance to the bulk (ABLDecorator.hpp:116-135 of the reference).
     AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE amrex::Real sigma(const amrex::IntVect& idx) const {
-        if (bulk.contains(idx)) return 0.0;
         int d2 = 0;
         for (int d = 0; d < 3; ++d) {
             const int v = idx[d] - amrex::Clamp(idx[d], bulk.smallEnd(d), bulk.bigEnd(d));
             d2 += v * v;
         }
+        if (d2 == 0) return 0.0;
         const amrex::Real dist = std::sqrt(static_cast<amrex::Real>(d2));
         const amrex::Real s = amrex::Clamp(data.inv_thickness * dist, 0.0, 1.0);
         return data.max_strength * data.profile(s);

@@ -44,7 +44,9 @@ kreiss_oliger(const amrex::Array4<ArrayType>& arr, int comp, const amrex::IntVec
         acc += c * (arr(i + s * U::x, j + s * U::y, k + s * U::z, comp) +
                     arr(i - s * U::x, j - s * U::y, k - s * U::z, comp));
     });
-    return acc * V(norm) * V(gf);
+    // one multiply by norm * gf: norm is a power of two, so this rounds exactly like
+    // (acc * norm) * gf
+    return acc * V(norm * gf);
 }
 
 template <int order, int d, typename ArrayType>

@@ -90,7 +90,18 @@ void run_steps(const ts_wave_desc& d, const RHS& rhs, const BC& bc, double* stat
         sp.time = t_arg;
         sp.err = err;
         typename EpiRK4<s>::Params ep{new_, argn, old_, L, dt * b_frac[s], dt * a_frac[(s + 1) % 4]};
-        Launcher::launch(tm, sp, rhs, ep, shape, stream);
+        CUtensorMap cmap[2];
+        int nmap = 0;
+        const CentreMaps cm = Launcher::centre_maps(
+            [&](const void* b, const Layout& Lc, int dtype, int bx, int by) -> const CUtensorMap& {
+                CUtensorMap& m = cmap[nmap++ & 1];
+                const ts_field_layout c = Lc.to_c(dtype);
+                if (ts_field_tensor_map(&c, b, bx, by, &m) != TS_OK)
+                    throw std::runtime_error("ts_field_tensor_map failed");
+                return m;
+            },
+            ep, shape);
+        Launcher::launch(tm, cm, sp, rhs, ep, shape, stream);
     };
 
     for (int n = 0; n < nsteps; ++n) {
