@@ -141,3 +141,37 @@ def test_fp32_stage_error_vs_fp64(ctx, bcmode):
     ctx.sync()
     e = relerr(out[TS_F32_STAGE], out[TS_F64])
     assert e <= 1e-6, e
+
+
+@pytest.mark.parametrize("precision", [TS_F64, TS_F32_STAGE])
+def test_static_ghost_fills_run_once_per_buffer(ctx, port_oracle, precision):
+    """Non-periodic Dirichlet data: each buffer's ghost cells are filled once, later fills skipped.
+
+    RK4 FP64: step 1 fills u, arg (twice: two stage buffers) = 3 fills + 4 stages; step 2 fills
+    the other state buffer = 1 + 4; from step 3 on only the 4 stage kernels run. A periodic
+    direction keeps every fill (4 + 4). The results still match the oracle.
+    """
+    n = (36, 30, 34)
+    mk = lambda periodic: wave_desc(n, 2, periodic=periodic, ko=0.1, bc=TS_BC_DIRICHLET, bc_values=(0.0, 0.0),
+                                    precision=precision, dt=0.2 / 36)
+    state = smooth_state((2, n[2], n[1], n[0]), seed=5)
+    d = mk((0, 0, 0))
+    it = Integrator(ctx, d)
+    it.set_state(state)
+    counts = []
+    for _ in range(4):
+        it.step(1)
+        ctx.sync()
+        counts.append(it.last_step_timing()[1])
+    want = [7, 5, 4, 4] if precision == TS_F64 else [4 + 4, 4 + 1, 4, 4]
+    assert counts == want, counts
+    gpu = it.get_state()
+    if precision == TS_F64:
+        cpu, _, _ = port_oracle.run(d, 4, state=state)
+        assert relerr(gpu, cpu) <= TOL_F64
+    it_p = Integrator(ctx, mk((1, 0, 0)))
+    it_p.set_state(state)
+    it_p.step(1)
+    it_p.step(1)
+    ctx.sync()
+    assert it_p.last_step_timing()[1] == 8

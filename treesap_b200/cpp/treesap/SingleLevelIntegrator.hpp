@@ -61,15 +61,30 @@ struct KernelClock {
 
 namespace detail {
 /// Tile shape of the fused stage kernel for a value type, ghost width and component count:
-/// 32-wide rows (one warp each), up to 7 rows plus the producer warp (256 threads, two CTAs
-/// per SM within the register file) with up to P = 4 planes of prefetch (fewer when the ring,
-/// including two FP64 centre-operand boxes per slot, would not leave room for two CTAs per
-/// SM); fewer rows and one CTA per SM for many components.
+/// CX cells per thread along x, TY rows (consumer warps) plus the producer warp, P planes of
+/// prefetch, MINB CTAs per SM, U planes per iteration; TREESAP_B200_TILE_F64 / _F32 override
+/// the defaults at build time as the decimal number CX TY(2 digits) P MINB U, e.g. 107222;
+/// when two FP64 centre-operand fields would not fit the shared-memory budget (many
+/// components), narrower tiles.
+#ifndef TREESAP_B200_TILE_F64
+#define TREESAP_B200_TILE_F64 107421
+#endif
+#ifndef TREESAP_B200_TILE_F32
+#define TREESAP_B200_TILE_F32 207421
+#endif
+template <int code> struct TileSpec {
+    static constexpr int CX = code / 100000, TY = code / 1000 % 100, P = code / 100 % 10, MINB = code / 10 % 10,
+                         U = code % 10;
+};
 template <typename T, int G, int NC> struct DefaultTile {
-    template <int TY, int P, int MINB = 2> using C = treesap_b200::TileCfg<32, TY, G, NC, T, P, MINB>;
-    using type = std::conditional_t<
-        C<7, 4>::fits, C<7, 4>,
-        std::conditional_t<C<3, 2>::fits, C<3, 2>, std::conditional_t<C<3, 2, 1>::fits, C<3, 2, 1>, C<1, 1, 1>>>>;
+    using Spec = std::conditional_t<sizeof(T) == 8, TileSpec<TREESAP_B200_TILE_F64>, TileSpec<TREESAP_B200_TILE_F32>>;
+    template <int CX, int TY, int P, int MINB, int U> using C = treesap_b200::TileCfg<CX, TY, G, NC, T, P, MINB, U>;
+    using Pref = C<Spec::CX, Spec::TY, Spec::P, Spec::MINB, Spec::U>;
+    using type =
+        std::conditional_t<Pref::fits, Pref,
+                           std::conditional_t<C<1, 3, 2, 2, 1>::fits, C<1, 3, 2, 2, 1>,
+                                              std::conditional_t<C<1, 3, 2, 1, 1>::fits, C<1, 3, 2, 1, 1>,
+                                                                 C<1, 1, 1, 1, 1>>>>;
 };
 } // namespace detail
 
@@ -134,6 +149,7 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
 
     void pre_step() final override {
         if (exporter) exporter->exportIfNecessary(int(steps), time);
+        fills_this_step_ = 0;
         FillPatch(state_old, time);
     }
 
@@ -204,10 +220,32 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
   protected:
     virtual amrex::Real computeNewState(amrex::Real dt_hint) = 0;
 
+    /// Ghost cells outside a non-periodic domain are never written by the stage kernels, so
+    /// when no direction is periodic and the BC functor's values depend neither on time nor on
+    /// the valid cells (BCType::is_time_independent and BCType::is_interior_independent), the
+    /// ghost cells of a buffer keep the values of its first fill: later fills are skipped.
+    static constexpr bool static_ghost_values =
+        requires { requires BCType::is_time_independent && BCType::is_interior_independent; };
+    bool ghosts_are_static() const {
+        return static_ghost_values && !(geom.is_periodic[0] || geom.is_periodic[1] || geom.is_periodic[2]);
+    }
+    /// Whether a ghost fill of buffer `buf` must be enqueued now (records it as filled).
+    bool ghost_fill_needed(const void* buf) {
+        if (!ghosts_are_static()) return true;
+        for (const void* p : ghosts_filled_)
+            if (p == buf) return false;
+        ghosts_filled_.push_back(buf);
+        return true;
+    }
+    /// Counts an enqueued ghost fill towards launches_per_step().
+    void count_fill() { ++fills_this_step_; }
+
     /// Ghost fill of an FP64 field with the model's BC functor (SingleLevelIntegrator.hpp:153-163).
     void FillPatch(Field& f, amrex::Real time_) {
         ScopedTimer timer("Integrator::FillPatch()");
         if (dry_run_) return;
+        if (!ghost_fill_needed(f.data())) return;
+        count_fill();
         clock_begin(0);
         treesap_b200::launch_ghost_fill(f.data(), f.layout(), geom, model.get_bc(), bc_recs_dev, time_,
                                         treesap_b200::GhostMode::Functor, sm_count(), stream());
@@ -253,6 +291,8 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
     double* staging = nullptr;
     treesap_b200::TensorMapCache tmaps;
     long long launches_per_step_ = 0;
+    long long fills_this_step_ = 0;          // ghost fills enqueued by the current step
+    std::vector<const void*> ghosts_filled_; // buffers whose static ghost cells are filled
     bool dry_run_ = false; // true while step_host_only() runs: no kernel launches
     KernelClock* clock_ = nullptr;
     void clock_begin(int cls) {

@@ -50,47 +50,68 @@ namespace treesap_b200 {
 
 constexpr int align128(int b) { return (b + 127) / 128 * 128; }
 
-template <int TX_, int TYMAX_, int G_, int NC_, typename T_, int P_ = 2, int MINB_ = 2> struct TileCfg {
+/// Tile configuration of the stage kernel: CX cells per thread along x (a warp covers
+/// TX = 32 CX cells of a row), up to TYMAX rows (consumer warps), ghost width G, NC components
+/// of type T, up to P planes of prefetch, MINB resident CTAs per SM, U planes per iteration of
+/// the plane loop.
+template <int CX_, int TYMAX_, int G_, int NC_, typename T_, int P_ = 2, int MINB_ = 2, int U_ = 1> struct TileCfg {
     using T = T_;
-    static constexpr int TX = TX_, TYMAX = TYMAX_, G = G_, NC = NC_, P = P_;
+    static constexpr int CX = CX_, TX = 32 * CX_, TYMAX = TYMAX_, G = G_, NC = NC_, P = P_, U = U_;
     static constexpr int MIN_BLOCKS = MINB_; // resident CTAs per SM the register and smem budgets are sized for
     static constexpr int A = 16 / int(sizeof(T));   // elements per 16 bytes
     static constexpr int XH = (G + A - 1) / A * A;  // x halo width in shared memory (16-byte aligned)
     static constexpr int BX = TX + 2 * XH;
     static constexpr int BYMAX = TYMAX + 2 * G;
     static constexpr int PLANE_MAX = NC * BYMAX * BX;  // stencil elements per slot (at TYMAX)
-    static constexpr int THREADS = TX * TYMAX + 32;    // consumer warps + one producer warp
+    static constexpr int THREADS = 32 * TYMAX + 32;    // consumer warps + one producer warp
     static constexpr int STENCIL_BYTES = align128(PLANE_MAX * int(sizeof(T)));
     static constexpr int CBOX = NC * TYMAX * TX;       // elements of one centre-operand box
     /// Dynamic shared memory per CTA when MIN_BLOCKS CTAs share an SM (228 KB per SM with 1 KB
     /// reserved per CTA; at most 227 KB for one CTA).
     static constexpr int SMEM_BUDGET = MINB_ == 1 ? 232448 : 233472 / MINB_ - 1024;
-    /// Ring slots of a given slot size: G + 1 + P, or fewer when the budget is smaller.
-    static constexpr int ring_slots(int slot_bytes) {
-        const int r = SMEM_BUDGET / (slot_bytes + 16);
-        return r < G + 1 + P ? r : G + 1 + P;
+    /// Shared memory of a stencil ring of G + U + p slots and a centre-operand ring of U + p
+    /// slots of `cslot` bytes (none when cslot = 0), with their mbarriers.
+    static constexpr int smem_for(int p, int cslot) {
+        return (G + U + p) * (STENCIL_BYTES + 16) + (cslot > 0 ? (U + p) * (cslot + 8) : 0);
     }
-    /// Usable when even two FP64 centre-operand fields leave one plane of prefetch.
-    static constexpr bool fits = ring_slots(STENCIL_BYTES + 2 * align128(CBOX * 8)) >= G + 2;
-    static_assert(TX == 32, "one warp per tile row");
+    /// Usable when even two FP64 centre-operand fields fit with one plane of prefetch.
+    static constexpr bool fits = smem_for(1, 2 * align128(CBOX * 8)) <= SMEM_BUDGET;
+    static_assert(CX == 1 || CX == 2, "one or two cells per thread along x");
+    static_assert(U == 1 || U == 2, "one or two planes per iteration");
     static_assert(BX <= 256 && BYMAX <= 256 && NC <= 256, "TMA box dimensions are limited to 256");
     static_assert(THREADS <= 1024, "too many threads");
 };
 
-/// Shared-memory ring of one (tile configuration, epilogue) pair. A slot holds the stencil
-/// plane ([comp][y][x], TY + 2G rows of BX) followed by the epilogue's centre-operand boxes
-/// ([comp][y][x], TY rows of TX), each 128-byte aligned.
+/// Shared-memory rings of one (tile configuration, epilogue) pair:
+///   * the stencil ring, R = G + U + P slots, each one stencil plane ([comp][y][x], TY + 2G
+///     rows of BX), with a `full` and an `empty` mbarrier per slot;
+///   * the centre-operand ring, RC = U + P slots (none without centre operands), each the
+///     epilogue's centre-operand boxes of one centre plane ([comp][y][x], TY rows of TX per
+///     field, 128-byte aligned), with an `empty` mbarrier per slot. The boxes of centre plane
+///     c are copied together with (and complete on the `full` barrier of) stencil plane c + G,
+///     the newest plane of the iteration that computes centre plane c.
+/// P is the configuration's prefetch depth, reduced until both rings fit the budget.
 template <class Cfg, class Epi> struct Ring {
     using C0 = typename Epi::C0;
     using C1 = typename Epi::C1;
     static constexpr int NCEN = Epi::kCentre;
     static_assert(NCEN >= 0 && NCEN <= 2, "at most two centre-operand fields");
-    static constexpr int C0_OFF = Cfg::STENCIL_BYTES;
-    static constexpr int C1_OFF = C0_OFF + (NCEN > 0 ? align128(Cfg::CBOX * int(sizeof(C0))) : 0);
-    static constexpr int SLOT = C1_OFF + (NCEN > 1 ? align128(Cfg::CBOX * int(sizeof(C1))) : 0);
-    static constexpr int R = Cfg::ring_slots(SLOT);
-    static constexpr int SMEM = R * SLOT + 16 * R;
-    static_assert(R >= Cfg::G + 2, "shared-memory ring too small for this tile configuration");
+    static constexpr int SSLOT = Cfg::STENCIL_BYTES;
+    static constexpr int C0_OFF = 0; // within a centre slot
+    static constexpr int C1_OFF = NCEN > 0 ? align128(Cfg::CBOX * int(sizeof(C0))) : 0;
+    static constexpr int CSLOT = NCEN > 1 ? C1_OFF + align128(Cfg::CBOX * int(sizeof(C1))) : C1_OFF;
+    static constexpr int P = [] {
+        int p = Cfg::P;
+        while (p > 1 && Cfg::smem_for(p, CSLOT) > Cfg::SMEM_BUDGET) --p;
+        return p;
+    }();
+    static constexpr int R = Cfg::G + Cfg::U + P;
+    static constexpr int RC = NCEN > 0 ? Cfg::U + P : 0;
+    static constexpr int CRING_OFF = R * SSLOT;             // centre ring
+    static constexpr int BAR_OFF = CRING_OFF + RC * CSLOT;  // full[R], empty[R], cempty[RC]
+    static constexpr int SMEM = BAR_OFF + 8 * (2 * R + RC);
+    static_assert(Cfg::smem_for(P, CSLOT) <= Cfg::SMEM_BUDGET,
+                  "shared-memory rings too large for this tile configuration");
 };
 
 /// Launch-invariant stage inputs.
@@ -126,6 +147,52 @@ struct CentreSrc {
     int dtype; // ts_dtype
 };
 
+/// Slot and completion parity of a plane in a ring of R slots, advanced plane by plane.
+struct RingPos {
+    int s = 0;
+    uint32_t ph = 0;
+    __device__ __forceinline__ void next(int R) {
+        if (++s == R) {
+            s = 0;
+            ph ^= 1u;
+        }
+    }
+};
+
+/// CX consecutive elements from shared memory (one vector load for CX = 2; 2 CX-element alignment).
+template <int CX, class V> __device__ __forceinline__ void lds(const V* p, V (&out)[CX]) {
+    if constexpr (CX == 2 && sizeof(V) == 8) {
+        const double2 v = *reinterpret_cast<const double2*>(p);
+        out[0] = v.x;
+        out[1] = v.y;
+    } else if constexpr (CX == 2 && sizeof(V) == 4) {
+        const float2 v = *reinterpret_cast<const float2*>(p);
+        out[0] = v.x;
+        out[1] = v.y;
+    } else {
+#pragma unroll
+        for (int e = 0; e < CX; ++e) out[e] = p[e];
+    }
+}
+
+/// Streaming store of CX consecutive cells, skipping inactive ones (one vector store when all
+/// CX are active; the address of cell 0 is aligned to CX elements).
+template <int CX, class V>
+__device__ __forceinline__ void stcs(V* p, const V (&v)[CX], const bool (&act)[CX]) {
+    if constexpr (CX == 2) {
+        if (act[0] && act[1]) {
+            if constexpr (sizeof(V) == 8)
+                __stcs(reinterpret_cast<double2*>(p), make_double2(v[0], v[1]));
+            else
+                __stcs(reinterpret_cast<float2*>(p), make_float2(v[0], v[1]));
+            return;
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < CX; ++e)
+        if (act[e]) __stcs(p + e, v[e]);
+}
+
 template <class Cfg, class RHS, class Epi>
 __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
     stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CentreMaps cmaps,
@@ -135,16 +202,18 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
     using C0 = typename RingT::C0;
     using C1 = typename RingT::C1;
     constexpr int G = Cfg::G, NC = Cfg::NC, TX = Cfg::TX, BX = Cfg::BX, XH = Cfg::XH;
-    constexpr int R = RingT::R, SLOT = RingT::SLOT, NCEN = RingT::NCEN;
+    constexpr int R = RingT::R, RC = RingT::RC, SSLOT = RingT::SSLOT, CSLOT = RingT::CSLOT, NCEN = RingT::NCEN;
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + R * SLOT);
+    unsigned char* cring = smem_raw + RingT::CRING_OFF;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + RingT::BAR_OFF);
     uint64_t* empty = full + R;
+    uint64_t* cempty = empty + R;
 
     const int TY = sp.ty;
     const int BY = TY + 2 * G;
     const int PNS = BY * BX; // component stride of the stencil plane inside a slot
-    const int CPS = TY * TX; // component stride of a centre-operand box inside a slot
+    const int CPS = TY * TX; // component stride of a centre-operand box
     const int ntiles = sp.ntx * sp.nty;
     const int tile = blockIdx.x % ntiles;
     const int z0 = (blockIdx.x / ntiles) * sp.zchunk;
@@ -159,6 +228,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
             ptx::mbar_init(&full[s], 1);
             ptx::mbar_init(&empty[s], uint32_t(TY));
         }
+        for (int s = 0; s < RC; ++s) ptx::mbar_init(&cempty[s], uint32_t(TY));
         ptx::fence_mbar_init();
     }
     __syncthreads();
@@ -173,31 +243,32 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
             uint32_t cbytes = 0;
             if constexpr (NCEN > 0) cbytes += uint32_t(NC * TY * TX * int(sizeof(C0)));
             if constexpr (NCEN > 1) cbytes += uint32_t(NC * TY * TX * int(sizeof(C1)));
-            // slot s of plane q; before refilling it, wait for completion q / R of empty[s]
-            // (parity (q / R - 1) & 1), i.e. the release of plane q - R
-            int q = 0, s = 0;
-            uint32_t ph = 1;
+            // Plane q goes to stencil slot ps.s once plane q - R is released (completion q / R
+            // of empty[ps.s], parity ps.ph ^ 1). From q = 2G on, the same transaction carries
+            // the centre operands of centre plane q - G (z = z0 - 2G + q) into centre slot
+            // pc.s, once the centre plane RC earlier has been released.
+            RingPos ps, pc;
+            int q = 0;
             for (; q < NP; ++q) {
-                if (q >= R && !ptx::mbar_wait(&empty[s], ph, sp.err)) break;
-                const int zq = z0 - G + q;
-                const bool centre = NCEN > 0 && zq >= z0 && zq < z1;
-                unsigned char* slot = smem_raw + s * SLOT;
-                ptx::mbar_arrive_expect_tx(&full[s], bytes + (centre ? cbytes : 0u));
-                // storage coordinates: x = x0 - XH + xoff (= x0), y = y0 - G + g (= y0), z = zq + g
-                ptx::tma_load_4d(slot, &tmap, x0, y0, z0 + q, 0, &full[s]);
+                if (q >= R && !ptx::mbar_wait(&empty[ps.s], ps.ph ^ 1u, sp.err)) break;
+                const bool centre = NCEN > 0 && q >= 2 * G;
+                if (centre && q - 2 * G >= RC && !ptx::mbar_wait(&cempty[pc.s], pc.ph ^ 1u, sp.err)) break;
+                ptx::mbar_arrive_expect_tx(&full[ps.s], bytes + (centre ? cbytes : 0u));
+                // storage coordinates: x = x0 - XH + xoff (= x0), y = y0 - G + g (= y0), z = z0 - G + q + g
+                ptx::tma_load_4d(smem_raw + ps.s * SSLOT, &tmap, x0, y0, z0 + q, 0, &full[ps.s]);
                 if constexpr (NCEN > 0) {
                     if (centre) {
-                        ptx::tma_load_4d(slot + RingT::C0_OFF, &cmaps.map[0], x0 + cmaps.x[0], y0 + cmaps.y[0],
-                                         zq + cmaps.z[0], 0, &full[s]);
+                        const int zc = z0 - 2 * G + q;
+                        unsigned char* cs = cring + pc.s * CSLOT;
+                        ptx::tma_load_4d(cs + RingT::C0_OFF, &cmaps.map[0], x0 + cmaps.x[0], y0 + cmaps.y[0],
+                                         zc + cmaps.z[0], 0, &full[ps.s]);
                         if constexpr (NCEN > 1)
-                            ptx::tma_load_4d(slot + RingT::C1_OFF, &cmaps.map[1], x0 + cmaps.x[1],
-                                             y0 + cmaps.y[1], zq + cmaps.z[1], 0, &full[s]);
+                            ptx::tma_load_4d(cs + RingT::C1_OFF, &cmaps.map[1], x0 + cmaps.x[1], y0 + cmaps.y[1],
+                                             zc + cmaps.z[1], 0, &full[ps.s]);
+                        pc.next(RC);
                     }
                 }
-                if (++s == R) {
-                    s = 0;
-                    ph ^= 1u;
-                }
+                ps.next(R);
             }
             if (q < NP) {
                 // a consumer warp stopped releasing slots: let the copies in flight land
@@ -219,72 +290,155 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
     const double time = sp.time;
     const typename Epi::Params epl = ep;
 
+    constexpr int CX = Cfg::CX, U = Cfg::U;
+    constexpr int QL = 2 * G + U; // register queue depth (planes)
     const int tx = lane, ty = warp;
-    const int i = x0 + tx, j = y0 + ty;
-    const bool active = (i < L.n[0]) && (j < L.n[1]);
-    const int coff = (ty + G) * BX + (tx + XH); // this thread's centre inside the stencil plane
-    const int cc = ty * TX + tx;                // ... inside a centre-operand box
-
-    T q[(2 * G + 1) * NC]; // register queue: q[(dk + G) * NC + c]
+    const int i0 = x0 + CX * tx, j = y0 + ty; // this thread's cells: (i0 + e, j), e < CX
+    bool act[CX];
 #pragma unroll
-    for (int e = 0; e < (2 * G + 1) * NC; ++e) q[e] = T(0);
+    for (int e = 0; e < CX; ++e) act[e] = (i0 + e < L.n[0]) && (j < L.n[1]);
+    const int coff = (ty + G) * BX + (CX * tx + XH); // cell 0's centre inside the stencil plane
+    const int cc = ty * TX + CX * tx;                // ... inside a centre-operand box
 
-    const T* in_col = sp.in + L.index(i, j, 0, 0); // global fallback: this column at z = 0
+    // q[e][m * NC + c]: column of cell e, plane it - 2G - U + m (before the shift of iteration it)
+    T q[CX][QL * NC];
+#pragma unroll
+    for (int e = 0; e < CX; ++e)
+#pragma unroll
+        for (int m = 0; m < QL * NC; ++m) q[e][m] = T(0);
+
+    const T* in_col = sp.in + L.index(i0, j, 0, 0); // global fallback: cell 0's column at z = 0
     const long long plane = L.px * L.py;
 
-    // s: slot of plane it (full-barrier parity ph); sc: slot of plane it - G, the stencil centre
-    // plane of iteration it. Plane p is released after iteration p (p < G: halo planes below the
-    // chunk) or p + G (its use as a centre plane); the last G planes need no release, since no
-    // copy waits for their slots.
-    int s = 0, sc = R - G;
-    uint32_t ph = 0;
-    for (int it = 0; it < NP; ++it) {
-        if (!ptx::mbar_wait(&full[s], ph, sp.err)) break;
-        const T* newest = reinterpret_cast<const T*>(smem_raw + s * SLOT);
+    // Prologue: planes 0 .. 2G-1 (the chunk's lower halo and first G centre planes) into the
+    // queue; planes below the chunk (p < G) are released at once.
+    RingPos pos; // plane it
+    bool ok = true;
 #pragma unroll
-        for (int e = 0; e < 2 * G * NC; ++e) q[e] = q[e + NC];
+    for (int p = 0; p < 2 * G; ++p) {
+        if (ok && !ptx::mbar_wait(&full[pos.s], pos.ph, sp.err)) ok = false;
+        if (ok) {
+            const T* pl = reinterpret_cast<const T*>(smem_raw + pos.s * SSLOT) + coff;
 #pragma unroll
-        for (int c = 0; c < NC; ++c) q[2 * G * NC + c] = newest[c * PNS + coff];
+            for (int c = 0; c < NC; ++c) {
+                T v[CX];
+                lds<CX>(pl + c * PNS, v);
+#pragma unroll
+                for (int e = 0; e < CX; ++e) q[e][(p + U) * NC + c] = v[e];
+            }
+            if (p < G) {
+                __syncwarp();
+                if (lane == 0) ptx::mbar_arrive(&empty[pos.s]);
+            }
+        }
+        pos.next(R);
+    }
+    if (!ok) return;
 
-        if (it >= 2 * G && active) {
-            const int z = z0 - 2 * G + it;
-            const unsigned char* cslot = smem_raw + sc * SLOT;
-            const T* ctr = reinterpret_cast<const T*>(cslot) + coff;
-            const CentreOps<C0, C1> co{reinterpret_cast<const C0*>(cslot + RingT::C0_OFF) + cc,
-                                       reinterpret_cast<const C1*>(cslot + RingT::C1_OFF) + cc, CPS};
-            amrex::StencilView<T> view{ctr, q, in_col + z * plane, L.px, plane, L.comp_stride(), i, j, z, BX, PNS,
-                                       G, NC};
-            amrex::Array4<const T> arr = make_array4<const T>(sp.in, L);
-            arr.view = &view;
-            typename RHS::Workspace ws{};
-            T kv[NC];
-            const amrex::IntVect idx{i, j, z};
-            treesap::static_for<NC>([&]<int c>() {
-                kv[c] = static_cast<T>(f.template operator()<c>(idx, time, arr, geom, ws));
-            });
-            Epi::template apply<T, NC>(epl, kv, ctr, PNS, i, j, z, co);
+    // Main loop: U planes per iteration. Cell (e, u) has centre plane it - G + u, i.e.
+    // z = z0 - 2G + it + u, and exists while it + u < NP; its queue window is q[e][u ...] and
+    // its centre operands are centre slot number it - 2G + u. After the iteration its centre
+    // plane and centre slot are released; the last G stencil planes need no release, since no
+    // copy waits for their slots.
+    RingPos cpos; // stencil slot of plane it - G
+    cpos.s = G;
+    RingPos kpos; // centre slot of centre plane it - G
+    for (int it = 2 * G; it < NP; it += U) {
+        int su[U], scu[U], sku[U];
+        {
+            RingPos pp = pos, cp = cpos, kp = kpos;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                su[u] = pp.s;
+                scu[u] = cp.s;
+                sku[u] = kp.s;
+                if (it + u < NP && !ptx::mbar_wait(&full[pp.s], pp.ph, sp.err)) ok = false;
+                pp.next(R);
+                cp.next(R);
+                if constexpr (NCEN > 0) kp.next(RC);
+            }
+        }
+        if (!ok) break;
+#pragma unroll
+        for (int e = 0; e < CX; ++e)
+#pragma unroll
+            for (int m = 0; m < 2 * G * NC; ++m) q[e][m] = q[e][m + U * NC];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (U == 1 || it + u < NP) {
+                const T* pl = reinterpret_cast<const T*>(smem_raw + su[u] * SSLOT) + coff;
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    T v[CX];
+                    lds<CX>(pl + c * PNS, v);
+#pragma unroll
+                    for (int e = 0; e < CX; ++e) q[e][(2 * G + u) * NC + c] = v[e];
+                }
+            }
+        }
+
+        // all cells' stage values first, then the epilogues (their global stores would
+        // otherwise stand between the shared-memory taps of neighbouring cells)
+        T kv[U][CX][NC];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int z = z0 - 2 * G + it + u;
+            const T* ctr = reinterpret_cast<const T*>(smem_raw + scu[u] * SSLOT) + coff;
+#pragma unroll
+            for (int e = 0; e < CX; ++e) {
+#pragma unroll
+                for (int c = 0; c < NC; ++c) kv[u][e][c] = T(0);
+                if ((U == 1 || it + u < NP) && act[e]) {
+                    amrex::StencilView<T> view{ctr + e,       q[e] + u * NC, in_col + e + z * plane, L.px, plane,
+                                               L.comp_stride(), i0 + e,      j, z, BX, PNS, G, NC};
+                    amrex::Array4<const T> arr = make_array4<const T>(sp.in, L);
+                    arr.view = &view;
+                    typename RHS::Workspace ws{};
+                    const amrex::IntVect idx{i0 + e, j, z};
+                    treesap::static_for<NC>([&]<int c>() {
+                        kv[u][e][c] = static_cast<T>(f.template operator()<c>(idx, time, arr, geom, ws));
+                    });
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (U == 1 || it + u < NP) {
+                const int z = z0 - 2 * G + it + u;
+                const unsigned char* cslot = cring + sku[u] * CSLOT;
+                const CentreOps<C0, C1> co{reinterpret_cast<const C0*>(cslot + RingT::C0_OFF) + cc,
+                                           reinterpret_cast<const C1*>(cslot + RingT::C1_OFF) + cc, CPS};
+                Epi::template apply<T, NC, CX>(epl, kv[u], act,
+                                               reinterpret_cast<const T*>(smem_raw + scu[u] * SSLOT) + coff, PNS,
+                                               i0, j, z, co);
+            }
         }
         __syncwarp();
         if (lane == 0) {
-            if (it < G)
-                ptx::mbar_arrive(&empty[s]);
-            else if (it >= 2 * G)
-                ptx::mbar_arrive(&empty[sc]);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (U == 1 || it + u < NP) {
+                    ptx::mbar_arrive(&empty[scu[u]]);
+                    if constexpr (NCEN > 0) ptx::mbar_arrive(&cempty[sku[u]]);
+                }
         }
-        if (++s == R) {
-            s = 0;
-            ph ^= 1u;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            pos.next(R);
+            cpos.next(R);
+            if constexpr (NCEN > 0) kpos.next(RC);
         }
-        if (++sc == R) sc = 0;
     }
 }
 
 // ------------------------------------------------------------------ epilogues
 // Each policy: struct Params; kCentre (0..2) centre-operand fields of element types C0, C1,
 // described on the host by centre_src(params, k); and
-//   template <T, NC, CO> static void apply(params, k[NC], centre, pns, i, j, z, co)
-// where `centre` points at component 0 of the stencil input's centre in shared memory and
-// co.c0 / co.c1 at component 0 of the centre operands (component stride co.cps).
+//   template <T, NC, CX, CO> static void apply(params, k[CX][NC], act[CX], centre, pns, i0, j, z, co)
+// for the CX cells (i0 + e, j, z) of a thread (act[e]: the cell exists), where `centre` points
+// at component 0 of cell 0's stencil input in shared memory (cell e at centre + e, component
+// stride pns) and co.c0 / co.c1 at component 0 of cell 0's centre operands (component stride
+// co.cps). i0 is a multiple of CX, so the CX cells of a row form one aligned vector.
 
 /// Epilogue without centre operands.
 struct NoCentre {
@@ -314,21 +468,28 @@ template <int STAGE> struct EpiRK4 {
     static CentreSrc centre_src(const Params& p, int k) {
         return k == 0 ? CentreSrc{p.acc, p.L, TS_F64} : CentreSrc{p.init, p.L, TS_F64};
     }
-    template <class T, int NC, class CO>
-    static __device__ __forceinline__ void apply(const Params& p, const T (&k)[NC], const T* centre, int pns, int i,
-                                                 int j, int z, const CO& co) {
-        const long long o0 = p.L.index(i, j, z, 0), cs = p.L.comp_stride();
+    template <class T, int NC, int CX, class CO>
+    static __device__ __forceinline__ void apply(const Params& p, const T (&k)[CX][NC], const bool (&act)[CX],
+                                                 const T* centre, int pns, int i0, int j, int z, const CO& co) {
+        const long long o0 = p.L.index(i0, j, z, 0), cs = p.L.comp_stride();
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-            const long long o = o0 + c * cs;
+            double base_acc[CX], base_init[CX], acc[CX], next[CX];
             if constexpr (STAGE == 0) {
-                const double u0 = centre[c * pns];
-                __stcs(p.acc + o, u0 + p.b * k[c]);
-                __stcs(p.arg_next + o, u0 + p.a_next * k[c]);
+                lds<CX>(centre + c * pns, base_acc);
+#pragma unroll
+                for (int e = 0; e < CX; ++e) base_init[e] = base_acc[e];
             } else {
-                if constexpr (STAGE < 3) __stcs(p.arg_next + o, co.c1[c * co.cps] + p.a_next * k[c]);
-                __stcs(p.acc + o, co.c0[c * co.cps] + p.b * k[c]);
+                lds<CX>(co.c0 + c * co.cps, base_acc);
+                if constexpr (STAGE < 3) lds<CX>(co.c1 + c * co.cps, base_init);
             }
+#pragma unroll
+            for (int e = 0; e < CX; ++e) {
+                acc[e] = base_acc[e] + p.b * k[e][c];
+                if constexpr (STAGE < 3) next[e] = base_init[e] + p.a_next * k[e][c];
+            }
+            stcs<CX>(p.acc + o0 + c * cs, acc, act);
+            if constexpr (STAGE < 3) stcs<CX>(p.arg_next + o0 + c * cs, next, act);
         }
     }
 };
@@ -340,12 +501,18 @@ struct EpiEuler : NoCentre {
         Layout L;
         double dt;
     };
-    template <class T, int NC, class CO>
-    static __device__ __forceinline__ void apply(const Params& p, const T (&k)[NC], const T* centre, int pns, int i,
-                                                 int j, int z, const CO&) {
-        const long long o0 = p.L.index(i, j, z, 0), cs = p.L.comp_stride();
+    template <class T, int NC, int CX, class CO>
+    static __device__ __forceinline__ void apply(const Params& p, const T (&k)[CX][NC], const bool (&act)[CX],
+                                                 const T* centre, int pns, int i0, int j, int z, const CO&) {
+        const long long o0 = p.L.index(i0, j, z, 0), cs = p.L.comp_stride();
 #pragma unroll
-        for (int c = 0; c < NC; ++c) __stcs(p.out + o0 + c * cs, centre[c * pns] + p.dt * k[c]);
+        for (int c = 0; c < NC; ++c) {
+            double u[CX], out[CX];
+            lds<CX>(centre + c * pns, u);
+#pragma unroll
+            for (int e = 0; e < CX; ++e) out[e] = u[e] + p.dt * k[e][c];
+            stcs<CX>(p.out + o0 + c * cs, out, act);
+        }
     }
 };
 
@@ -365,14 +532,22 @@ struct EpiF32S0 : NoCentre {
         Layout Lu;
         double dt;
     };
-    template <class T, int NC, class CO>
-    static __device__ __forceinline__ void apply(const Params& p, const T (&k)[NC], const T* centre, int pns, int i,
-                                                 int j, int z, const CO&) {
-        const long long u0 = p.Lu.index(i, j, z, 0), us = p.Lu.comp_stride();
+    template <class T, int NC, int CX, class CO>
+    static __device__ __forceinline__ void apply(const Params& p, const T (&k)[CX][NC], const bool (&act)[CX],
+                                                 const T* centre, int pns, int i0, int j, int z, const CO&) {
+        const long long u0 = p.Lu.index(i0, j, z, 0), us = p.Lu.comp_stride();
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-            __stcs(p.k0 + u0 + c * us, double(k[c]));
-            __stcs(p.up + u0 + c * us, double(centre[c * pns]) + p.dt * double(k[c]));
+            T u[CX];
+            lds<CX>(centre + c * pns, u);
+            double k0[CX], up[CX];
+#pragma unroll
+            for (int e = 0; e < CX; ++e) {
+                k0[e] = double(k[e][c]);
+                up[e] = double(u[e]) + p.dt * double(k[e][c]);
+            }
+            stcs<CX>(p.k0 + u0 + c * us, k0, act);
+            stcs<CX>(p.up + u0 + c * us, up, act);
         }
     }
 };
@@ -384,12 +559,17 @@ struct EpiF32S1 : NoCentre {
         Layout Lf;
         double a_dt;
     };
-    template <class T, int NC, class CO>
-    static __device__ __forceinline__ void apply(const Params& p, const T (&lk)[NC], const T*, int, int i, int j,
-                                                 int z, const CO&) {
-        const long long o0 = p.Lf.index(i, j, z, 0), cs = p.Lf.comp_stride();
+    template <class T, int NC, int CX, class CO>
+    static __device__ __forceinline__ void apply(const Params& p, const T (&lk)[CX][NC], const bool (&act)[CX],
+                                                 const T*, int, int i0, int j, int z, const CO&) {
+        const long long o0 = p.Lf.index(i0, j, z, 0), cs = p.Lf.comp_stride();
 #pragma unroll
-        for (int c = 0; c < NC; ++c) p.d1[o0 + c * cs] = static_cast<float>(p.a_dt * double(lk[c]));
+        for (int c = 0; c < NC; ++c) {
+            float d[CX];
+#pragma unroll
+            for (int e = 0; e < CX; ++e) d[e] = static_cast<float>(p.a_dt * double(lk[e][c]));
+            stcs<CX>(p.d1 + o0 + c * cs, d, act);
+        }
     }
 };
 
@@ -410,24 +590,43 @@ template <int STAGE> struct EpiF32Lin {
     static CentreSrc centre_src(const Params& p, int k) {
         return k == 0 ? CentreSrc{p.d1, p.Lf, TS_F32} : CentreSrc{p.u, p.Lu, TS_F64};
     }
-    template <class T, int NC, class CO>
-    static __device__ __forceinline__ void apply(const Params& p, const T (&lk)[NC], const T* centre, int pns, int i,
-                                                 int j, int z, const CO& co) {
-        const long long o0 = p.Lf.index(i, j, z, 0), cs = p.Lf.comp_stride();
+    template <class T, int NC, int CX, class CO>
+    static __device__ __forceinline__ void apply(const Params& p, const T (&lk)[CX][NC], const bool (&act)[CX],
+                                                 const T* centre, int pns, int i0, int j, int z, const CO& co) {
+        const long long o0 = p.Lf.index(i0, j, z, 0), cs = p.Lf.comp_stride();
         if constexpr (STAGE == 1) {
 #pragma unroll
-            for (int c = 0; c < NC; ++c) p.d_out[o0 + c * cs] = p.a_dt * lk[c];
+            for (int c = 0; c < NC; ++c) {
+                float d[CX];
+#pragma unroll
+                for (int e = 0; e < CX; ++e) d[e] = p.a_dt * lk[e][c];
+                stcs<CX>(p.d_out + o0 + c * cs, d, act);
+            }
         } else if constexpr (STAGE == 2) {
 #pragma unroll
-            for (int c = 0; c < NC; ++c) p.d_out[o0 + c * cs] = centre[c * pns] + p.a_dt * lk[c];
+            for (int c = 0; c < NC; ++c) {
+                float d1[CX], d[CX];
+                lds<CX>(centre + c * pns, d1);
+#pragma unroll
+                for (int e = 0; e < CX; ++e) d[e] = d1[e] + p.a_dt * lk[e][c];
+                stcs<CX>(p.d_out + o0 + c * cs, d, act);
+            }
         } else {
-            const long long u0 = p.Lu.index(i, j, z, 0), us = p.Lu.comp_stride();
+            const long long u0 = p.Lu.index(i0, j, z, 0), us = p.Lu.comp_stride();
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
-                const float d1 = co.c0[c * co.cps], d2 = centre[c * pns];
-                const float d3 = 2.0f * d1 + p.a_dt * lk[c];
-                const double sum = 2.0 * double(d1) + 2.0 * double(d2) + double(d3);
-                __stcs(p.u + u0 + c * us, co.c1[c * co.cps] + (p.dt / 6.0) * sum);
+                float d1[CX], d2[CX];
+                double up[CX], un[CX];
+                lds<CX>(co.c0 + c * co.cps, d1);
+                lds<CX>(centre + c * pns, d2);
+                lds<CX>(co.c1 + c * co.cps, up);
+#pragma unroll
+                for (int e = 0; e < CX; ++e) {
+                    const float d3 = 2.0f * d1[e] + p.a_dt * lk[e][c];
+                    const double sum = 2.0 * double(d1[e]) + 2.0 * double(d2[e]) + double(d3);
+                    un[e] = up[e] + (p.dt / 6.0) * sum;
+                }
+                stcs<CX>(p.u + u0 + c * us, un, act);
             }
         }
     }

@@ -44,7 +44,7 @@ class SingleLevelEulerIntegrator : public SingleLevelIntegrator<PDEModelType> {
                              this->stream());
             this->clock_end();
         }
-        this->launches_per_step_ = 2;
+        this->launches_per_step_ = 1 + this->fills_this_step_;
         return delta_time;
     }
 };

@@ -55,7 +55,6 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
   protected:
     amrex::Real computeNewState(amrex::Real dt) override {
         using namespace treesap_b200;
-        this->launches_per_step_ = 4 + 4;
         if (this->dry_run_) return dt;
         const Layout& Lu = state_old.layout();
         const Layout& Lf = d1.layout();
@@ -100,6 +99,7 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
         lin_stage<2>(d1, d2, float(0.5 * dt), dt, err);
         fill_increment(d2);
         lin_stage<3>(d2, d2, float(dt), dt, err);
+        this->launches_per_step_ = 4 + this->fills_this_step_;
         return dt;
     }
 
@@ -131,6 +131,8 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
     }
 
     template <class F> void fill_increment(F& f) {
+        if (!this->ghost_fill_needed(f.data())) return;
+        this->count_fill();
         this->clock_begin(0);
         treesap_b200::launch_ghost_fill(f.data(), f.layout(), geom, model.get_bc(), this->bc_recs_dev, time,
                                         treesap_b200::GhostMode::Homogeneous, this->sm_count(), this->stream());

@@ -46,7 +46,7 @@ class SingleLevelRK4Integrator : public SingleLevelIntegrator<PDEModelType> {
         run_stage<1>(delta_time);
         run_stage<2>(delta_time);
         run_stage<3>(delta_time);
-        this->launches_per_step_ = 4 + 4; // 4 stages + 4 ghost fills (one in pre_step)
+        this->launches_per_step_ = 4 + this->fills_this_step_; // 4 stages + the ghost fills enqueued
         return delta_time;
     }
 

@@ -13,6 +13,8 @@ template <int ncomp_, int ngrow_> struct DirichletBC {
     static constexpr int ngrow = ngrow_;
     /// The boundary data do not depend on time (lets the FP32-stage form treat stage increments as homogeneous).
     static constexpr bool is_time_independent = true;
+    /// ... nor on the valid cells (lets the integrators fill static ghost cells once per buffer).
+    static constexpr bool is_interior_independent = true;
 
     amrex::GpuArray<amrex::Real, ncomp> boundary_values{};
 

@@ -10,6 +10,7 @@ template <int ncomp_, int ngrow_> struct NoOpBC {
     static constexpr int ncomp = ncomp_;
     static constexpr int ngrow = ngrow_;
     static constexpr bool is_time_independent = true;
+    static constexpr bool is_interior_independent = true;
 
     AMREX_GPU_HOST_DEVICE void operator()(amrex::IntVect const&, amrex::Array4<amrex::Real> const&, int, int,
                                           amrex::GeometryData const&, amrex::Real, const amrex::BCRec*, int,

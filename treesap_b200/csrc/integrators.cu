@@ -20,6 +20,7 @@ struct ts_integrator {
     // CUDA graphs of one step, for the two buffer parities (state and stage buffers swap every step)
     bool use_graph = false;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    long long graph_launches[2] = {0, 0}; // kernels in each captured step
     double graph_dt = 0.0;
 };
 
@@ -169,16 +170,18 @@ ts_status ts_integrator_step(ts_integrator* it, int nsteps) {
                     cuda_check(cudaStreamEndCapture(s, &g), "cudaStreamEndCapture");
                     cuda_check(cudaGraphInstantiate(&it->graph[parity], g, 0), "cudaGraphInstantiate");
                     cudaGraphDestroy(g);
+                    it->graph_launches[parity] = it->impl->launches_per_step();
                     // the capture ran the host bookkeeping (swaps, clock) but no device work: launch it once
                     cuda_check(cudaGraphLaunch(it->graph[parity], s), "cudaGraphLaunch");
                 } else {
                     cuda_check(cudaGraphLaunch(it->graph[parity], s), "cudaGraphLaunch");
                     it->impl->step_host_only();
                 }
+                launches += it->graph_launches[parity];
             } else {
                 it->impl->step();
+                launches += it->impl->launches_per_step();
             }
-            launches += it->impl->launches_per_step();
         }
         cuda_check(cudaEventRecord(it->ev1, s), "cudaEventRecord");
         it->last_launches = launches;
