@@ -151,7 +151,7 @@ def traffic_from_profiles(key: str):
     """DRAM bytes per launch of a kernel from the committed ncu summary (null when absent)."""
     try:
         t = json.loads((ROOT / "profiles" / "dram_traffic_c2_256.json").read_text())
-        return t.get(key)
+        return t.get("bytes", {}).get(key)
     except (OSError, ValueError):
         return None
 

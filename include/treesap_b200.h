@@ -166,6 +166,36 @@ TS_API ts_status ts_integrator_profile(ts_integrator* it, int nsteps, int nclass
  * the default shape is chosen per launch from the SM count and the domain. */
 TS_API ts_status ts_integrator_set_launch_shape(ts_integrator* it, int rows, int chunks);
 
+/* ------------------------------------------------------------------ batched instances
+ * No counterpart in the reference, which advances one model per integrator object: `count`
+ * independent instances of TS_MODEL_WAVE (each descriptor its own extents, geometry, dt,
+ * periodicity, boundary values and Kreiss-Oliger strength; all with the same ngrow (2 or 4),
+ * precision, scheme TS_RK4 and either all or none with Kreiss-Oliger; no absorbing layer, no
+ * c2) advanced together. Per RK4 stage ONE persistent launch of the fused stage kernel walks a
+ * work list of (instance, tile, z range) items; per ghost fill one launch covers all
+ * instances; with ts_batch_use_graph each step replays a captured CUDA graph. Results are
+ * bitwise identical to ts_integrator_* on each instance. TS_BC_NOOP ghost cells hold 0. */
+typedef struct ts_batch ts_batch;
+/* A batch (like an integrator) uses its context's stream: destroy it before the context. */
+TS_API ts_status ts_batch_create(ts_context* ctx, const ts_wave_desc* descs, int count, ts_batch** out);
+TS_API ts_status ts_batch_destroy(ts_batch* b);
+TS_API int ts_batch_size(const ts_batch* b);
+/* Like ts_integrator_initialise for one instance (at most 64 items). */
+TS_API ts_status ts_batch_initialise(ts_batch* b, int instance, int init_kind, int nitems, const double* items);
+TS_API ts_status ts_batch_set_state(ts_batch* b, int instance, const double* src, int src_is_device);
+TS_API ts_status ts_batch_get_state(ts_batch* b, int instance, double* dst, int dst_is_device);
+/* nsteps RK4 steps of every instance, enqueued on the context stream. */
+TS_API ts_status ts_batch_step(ts_batch* b, int nsteps);
+TS_API ts_status ts_batch_use_graph(ts_batch* b, int enable);
+/* Work-item shape: tile rows and z-range length in planes (0 = automatic: the largest tile,
+ * whole z extents). */
+TS_API ts_status ts_batch_set_launch_shape(ts_batch* b, int rows, int zchunk);
+/* Times candidate shapes on the batch itself (trial_steps steps each, states restored
+ * afterwards), keeps the fastest and returns it. */
+TS_API ts_status ts_batch_autotune(ts_batch* b, int trial_steps, int* rows, int* zchunk);
+/* Device time and kernel launches of the last ts_batch_step call (valid after ts_context_sync). */
+TS_API ts_status ts_batch_last_step_timing(ts_batch* b, double* ms, long long* launches);
+
 /* ------------------------------------------------------------------ allocation-free stepping
  * No counterpart in the reference. For callers that must not allocate device memory: host
  * applications that own all device memory through their own pool or arena, and loops that

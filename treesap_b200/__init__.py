@@ -8,6 +8,7 @@ loudly when the library has not been built.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from pathlib import Path
 
 import numpy as np
@@ -20,6 +21,7 @@ __all__ = [
     "lib",
     "Context",
     "Integrator",
+    "Batch",
     "TS_EULER",
     "TS_RK4",
     "TS_F64",
@@ -142,6 +144,17 @@ def lib() -> C.CDLL:
         "ts_integrator_last_step_timing": (i, [vp, C.POINTER(d), C.POINTER(ll)]),
         "ts_integrator_profile": (i, [vp, i, i, C.POINTER(ll), C.POINTER(d)]),
         "ts_integrator_set_launch_shape": (i, [vp, i, i]),
+        "ts_batch_create": (i, [vp, vp, i, C.POINTER(vp)]),
+        "ts_batch_destroy": (i, [vp]),
+        "ts_batch_size": (i, [vp]),
+        "ts_batch_initialise": (i, [vp, i, i, i, vp]),
+        "ts_batch_set_state": (i, [vp, i, vp, i]),
+        "ts_batch_get_state": (i, [vp, i, vp, i]),
+        "ts_batch_step": (i, [vp, i]),
+        "ts_batch_use_graph": (i, [vp, i]),
+        "ts_batch_set_launch_shape": (i, [vp, i, i]),
+        "ts_batch_autotune": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
+        "ts_batch_last_step_timing": (i, [vp, C.POINTER(d), C.POINTER(ll)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -164,7 +177,11 @@ class Context:
 
     def __init__(self, device: int = 0):
         self.handle = C.c_void_p()
+        self._dependents = weakref.WeakSet()  # integrators / batches, destroyed before the context
         _check(lib().ts_context_create(device, C.byref(self.handle)), "ts_context_create")
+
+    def _adopt(self, obj) -> None:
+        self._dependents.add(obj)
 
     def sync(self) -> None:
         _check(lib().ts_context_sync(self.handle), "ts_context_sync", self)
@@ -179,6 +196,8 @@ class Context:
 
     def close(self) -> None:
         if self.handle:
+            for dep in list(self._dependents):
+                dep.close()
             lib().ts_context_destroy(self.handle)
             self.handle = C.c_void_p()
 
@@ -201,6 +220,7 @@ class Integrator:
             desc.c2 = self._c2.ctypes.data
         self.handle = C.c_void_p()
         _check(lib().ts_integrator_create(ctx.handle, C.byref(desc), C.byref(self.handle)), "ts_integrator_create", ctx)
+        ctx._adopt(self)
         self.shape = desc.shape()
 
     def initialise(self, kind: int, items: np.ndarray) -> None:
@@ -267,6 +287,69 @@ class Integrator:
     def close(self) -> None:
         if self.handle:
             lib().ts_integrator_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Independent instances of the scalar wave model advanced together (ts_batch)."""
+
+    def __init__(self, ctx: Context, descs: list[WaveDesc]):
+        self.ctx = ctx
+        self.descs = (WaveDesc * len(descs))(*descs)
+        self.shapes = [d.shape() for d in descs]
+        self.handle = C.c_void_p()
+        _check(lib().ts_batch_create(ctx.handle, C.cast(self.descs, C.c_void_p), len(descs), C.byref(self.handle)),
+               "ts_batch_create", ctx)
+        ctx._adopt(self)
+
+    def __len__(self) -> int:
+        return lib().ts_batch_size(self.handle)
+
+    def initialise(self, instance: int, kind: int, items: np.ndarray) -> None:
+        items = np.ascontiguousarray(items, dtype=np.float64).reshape(-1, 6)
+        _check(lib().ts_batch_initialise(self.handle, instance, kind, len(items), items.ctypes.data),
+               "ts_batch_initialise", self.ctx)
+
+    def set_state(self, instance: int, state: np.ndarray) -> None:
+        a = np.ascontiguousarray(state, dtype=np.float64)
+        assert a.shape == self.shapes[instance], (a.shape, self.shapes[instance])
+        _check(lib().ts_batch_set_state(self.handle, instance, a.ctypes.data, 0), "ts_batch_set_state", self.ctx)
+        self.ctx.sync()
+
+    def get_state(self, instance: int) -> np.ndarray:
+        out = np.empty(self.shapes[instance], dtype=np.float64)
+        _check(lib().ts_batch_get_state(self.handle, instance, out.ctypes.data, 0), "ts_batch_get_state", self.ctx)
+        return out
+
+    def step(self, nsteps: int = 1) -> None:
+        _check(lib().ts_batch_step(self.handle, nsteps), "ts_batch_step", self.ctx)
+
+    def use_graph(self, enable: bool = True) -> None:
+        _check(lib().ts_batch_use_graph(self.handle, int(enable)), "ts_batch_use_graph", self.ctx)
+
+    def set_launch_shape(self, rows: int = 0, zchunk: int = 0) -> None:
+        _check(lib().ts_batch_set_launch_shape(self.handle, rows, zchunk), "ts_batch_set_launch_shape", self.ctx)
+
+    def autotune(self, trial_steps: int = 3) -> tuple[int, int]:
+        r, z = C.c_int(), C.c_int()
+        _check(lib().ts_batch_autotune(self.handle, trial_steps, C.byref(r), C.byref(z)), "ts_batch_autotune",
+               self.ctx)
+        return r.value, z.value
+
+    def last_step_timing(self) -> tuple[float, int]:
+        ms, n = C.c_double(), C.c_longlong()
+        _check(lib().ts_batch_last_step_timing(self.handle, C.byref(ms), C.byref(n)), "ts_batch_timing", self.ctx)
+        return ms.value, n.value
+
+    def close(self) -> None:
+        if self.handle:
+            lib().ts_batch_destroy(self.handle)
             self.handle = C.c_void_p()
 
     def __del__(self):

@@ -67,33 +67,69 @@ AMREX_GPU_HOST_DEVICE inline void ghost_coords(const Layout& L, long long t, int
     i = ii < g ? ii - g : n0 + (ii - g);
 }
 
+/// Fills ghost cell number t of field f (slab enumeration of ghost_coords).
+template <class T, class BC>
+__device__ __forceinline__ void ghost_fill_cell(T* __restrict__ f, const Layout& L, const amrex::GeometryData& geom,
+                                                const BC& bc, const amrex::BCRec* bcr, double time, int mode,
+                                                long long t) {
+    int i, j, k;
+    ghost_coords(L, t, i, j, k);
+    int s[3] = {i, j, k};
+    bool inside = true;
+    for (int d = 0; d < 3; ++d) {
+        if (geom.is_periodic[d]) s[d] = ((s[d] % L.n[d]) + L.n[d]) % L.n[d];
+        if (s[d] < 0 || s[d] >= L.n[d]) inside = false;
+    }
+    const long long cs = L.comp_stride();
+    if (inside) {
+        const long long dst = L.index(i, j, k, 0), src = L.index(s[0], s[1], s[2], 0);
+        for (int c = 0; c < L.nc; ++c) f[dst + c * cs] = f[src + c * cs];
+    } else if (mode == int(GhostMode::Homogeneous)) {
+        const long long dst = L.index(i, j, k, 0);
+        for (int c = 0; c < L.nc; ++c) f[dst + c * cs] = T(0);
+    } else if (mode == int(GhostMode::Functor)) {
+        if constexpr (std::is_same_v<T, amrex::Real>) {
+            const amrex::Array4<amrex::Real> dest = make_array4(f, L);
+            bc(amrex::IntVect{i, j, k}, dest, 0, L.nc, geom, time, bcr, 0, 0);
+        }
+    }
+}
+
 template <class T, class BC>
 __global__ void ghost_fill_kernel(T* __restrict__ f, const Layout L, const amrex::GeometryData geom, const BC bc,
                                   const amrex::BCRec* bcr, double time, int mode) {
     const long long total = ghost_count(L).total();
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x)
+        ghost_fill_cell(f, L, geom, bc, bcr, time, mode, t);
+}
+
+/// One field of a batched ghost fill; `first` = ghost cells of all earlier entries.
+template <class T, class BC> struct GhostEntry {
+    T* f;
+    Layout L;
+    amrex::GeometryData geom;
+    BC bc;
+    double time;
+    int mode;
+    long long first;
+};
+
+/// Ghost fill of many fields in one launch: thread t of the grid-stride loop fills ghost cell
+/// t - first of the entry whose range holds t (binary search over the entries' `first`).
+template <class T, class BC>
+__global__ void batch_ghost_fill_kernel(const GhostEntry<T, BC>* __restrict__ entries, int count, long long total,
+                                        const amrex::BCRec* bcr) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
-        int i, j, k;
-        ghost_coords(L, t, i, j, k);
-        int s[3] = {i, j, k};
-        bool inside = true;
-        for (int d = 0; d < 3; ++d) {
-            if (geom.is_periodic[d]) s[d] = ((s[d] % L.n[d]) + L.n[d]) % L.n[d];
-            if (s[d] < 0 || s[d] >= L.n[d]) inside = false;
+        int lo = 0, hi = count - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (entries[mid].first <= t) lo = mid;
+            else hi = mid - 1;
         }
-        const long long cs = L.comp_stride();
-        if (inside) {
-            const long long dst = L.index(i, j, k, 0), src = L.index(s[0], s[1], s[2], 0);
-            for (int c = 0; c < L.nc; ++c) f[dst + c * cs] = f[src + c * cs];
-        } else if (mode == int(GhostMode::Homogeneous)) {
-            const long long dst = L.index(i, j, k, 0);
-            for (int c = 0; c < L.nc; ++c) f[dst + c * cs] = T(0);
-        } else if (mode == int(GhostMode::Functor)) {
-            if constexpr (std::is_same_v<T, amrex::Real>) {
-                const amrex::Array4<amrex::Real> dest = make_array4(f, L);
-                bc(amrex::IntVect{i, j, k}, dest, 0, L.nc, geom, time, bcr, 0, 0);
-            }
-        }
+        const GhostEntry<T, BC>& e = entries[lo];
+        ghost_fill_cell(e.f, e.L, e.geom, e.bc, bcr, e.time, e.mode, t - e.first);
     }
 }
 

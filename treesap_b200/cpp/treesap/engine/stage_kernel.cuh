@@ -193,10 +193,76 @@ __device__ __forceinline__ void stcs(V* p, const V (&v)[CX], const bool (&act)[C
         if (act[e]) __stcs(p + e, v[e]);
 }
 
-template <class Cfg, class RHS, class Epi>
-__global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
-    stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CentreMaps cmaps,
-                 const StageParams<typename Cfg::T> sp, const RHS rhs, const typename Epi::Params ep) {
+/// One unit of work of a CTA: the tile at (x0, y0) of instance `inst`, planes z0 .. z1-1.
+struct ItemBox {
+    int inst, x0, y0, z0, z1;
+};
+
+/// Work source of a single-box launch: one item per CTA (tile blockIdx % ntiles, z chunk
+/// blockIdx / ntiles), everything else in kernel-parameter space.
+template <class Cfg, class RHS, class Epi> struct SingleSource {
+    using T = typename Cfg::T;
+    const CUtensorMap* tmap;
+    const CentreMaps* cmaps;
+    const StageParams<T>* sp;
+    const RHS* rhs;
+    const typename Epi::Params* ep;
+    __device__ __forceinline__ int ty() const { return sp->ty; }
+    __device__ __forceinline__ int* err() const { return sp->err; }
+    __device__ __forceinline__ ItemBox first() const {
+        const int ntiles = sp->ntx * sp->nty;
+        const int tile = blockIdx.x % ntiles;
+        const int z0 = (blockIdx.x / ntiles) * sp->zchunk;
+        return {0, (tile % sp->ntx) * Cfg::TX, (tile / sp->ntx) * sp->ty, z0, min(sp->L.n[2], z0 + sp->zchunk)};
+    }
+    __device__ __forceinline__ int count() const {
+        const ItemBox b = first();
+        return b.z0 < b.z1 ? 1 : 0;
+    }
+    __device__ __forceinline__ ItemBox item(int) const { return first(); }
+    __device__ __forceinline__ const CUtensorMap* stencil_map(int) const { return tmap; }
+    __device__ __forceinline__ const CentreMaps& centre_maps(int) const { return *cmaps; }
+    __device__ __forceinline__ const StageParams<T>& params(int) const { return *sp; }
+    __device__ __forceinline__ const RHS& rhs_of(int) const { return *rhs; }
+    __device__ __forceinline__ const typename Epi::Params& epi(int) const { return *ep; }
+};
+
+/// Per-instance data of a batched launch (global memory, 64-byte aligned for the descriptors).
+template <class Cfg, class RHS, class Epi> struct alignas(64) StageEntry {
+    CUtensorMap tmap;
+    CentreMaps cmaps;
+    StageParams<typename Cfg::T> sp; // ntx, nty, ty, zchunk unused
+    RHS rhs;
+    typename Epi::Params ep;
+};
+
+/// Work source of a persistent batched launch: CTA b processes items b, b + grid, b + 2 grid, ...
+/// of a host-built list (instances of any size, tiles x z ranges, longest first).
+template <class Cfg, class RHS, class Epi> struct BatchSource {
+    using T = typename Cfg::T;
+    using Entry = StageEntry<Cfg, RHS, Epi>;
+    const Entry* entries;
+    const ItemBox* items;
+    int nitems, ty_;
+    int* err_;
+    __device__ __forceinline__ int ty() const { return ty_; }
+    __device__ __forceinline__ int* err() const { return err_; }
+    __device__ __forceinline__ int count() const {
+        return int(blockIdx.x) < nitems ? (nitems - 1 - int(blockIdx.x)) / int(gridDim.x) + 1 : 0;
+    }
+    __device__ __forceinline__ ItemBox item(int m) const { return items[blockIdx.x + size_t(m) * gridDim.x]; }
+    __device__ __forceinline__ const CUtensorMap* stencil_map(int i) const { return &entries[i].tmap; }
+    __device__ __forceinline__ const CentreMaps& centre_maps(int i) const { return entries[i].cmaps; }
+    __device__ __forceinline__ const StageParams<T>& params(int i) const { return entries[i].sp; }
+    __device__ __forceinline__ const RHS& rhs_of(int i) const { return entries[i].rhs; }
+    __device__ __forceinline__ const typename Epi::Params& epi(int i) const { return entries[i].ep; }
+};
+
+/// The stage pipeline of one CTA over the items of a work source. The two rings run on across
+/// items: the producer streams the planes of item after item and the consumer warps follow in
+/// the same order, so an item's first planes are copied while the previous item's last
+/// planes are computed.
+template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__ void stage_body(const Src& src) {
     using T = typename Cfg::T;
     using RingT = Ring<Cfg, Epi>;
     using C0 = typename RingT::C0;
@@ -210,17 +276,13 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
     uint64_t* empty = full + R;
     uint64_t* cempty = empty + R;
 
-    const int TY = sp.ty;
+    const int TY = src.ty();
     const int BY = TY + 2 * G;
     const int PNS = BY * BX; // component stride of the stencil plane inside a slot
     const int CPS = TY * TX; // component stride of a centre-operand box
-    const int ntiles = sp.ntx * sp.nty;
-    const int tile = blockIdx.x % ntiles;
-    const int z0 = (blockIdx.x / ntiles) * sp.zchunk;
-    const int z1 = min(sp.L.n[2], z0 + sp.zchunk);
-    if (z0 >= z1) return;
-    const int NP = (z1 - z0) + 2 * G; // planes streamed: z0 - G .. z1 - 1 + G
-    const int x0 = (tile % sp.ntx) * TX, y0 = (tile / sp.ntx) * TY;
+    const int nitems = src.count();
+    if (nitems == 0) return;
+    int* const err = src.err();
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
 
     if (threadIdx.x == 0) {
@@ -236,43 +298,64 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
     if (warp == TY) {
         // ---------------------------------------------------------------- producer warp
         if (lane == 0) {
-            ptx::prefetch_tensor_map(&tmap);
-            if constexpr (NCEN > 0) ptx::prefetch_tensor_map(&cmaps.map[0]);
-            if constexpr (NCEN > 1) ptx::prefetch_tensor_map(&cmaps.map[1]);
             const uint32_t bytes = uint32_t(NC * BY * BX * int(sizeof(T)));
             uint32_t cbytes = 0;
             if constexpr (NCEN > 0) cbytes += uint32_t(NC * TY * TX * int(sizeof(C0)));
             if constexpr (NCEN > 1) cbytes += uint32_t(NC * TY * TX * int(sizeof(C1)));
-            // Plane q goes to stencil slot ps.s once plane q - R is released (completion q / R
-            // of empty[ps.s], parity ps.ph ^ 1). From q = 2G on, the same transaction carries
-            // the centre operands of centre plane q - G (z = z0 - 2G + q) into centre slot
-            // pc.s, once the centre plane RC earlier has been released.
+            // Plane t (counted over all items) goes to stencil slot ps.s once plane t - R is
+            // released (completion t / R of empty[ps.s], parity ps.ph ^ 1). From an item's plane
+            // q = 2G on, the same transaction carries the centre operands of its centre plane
+            // q - G (z = z0 - 2G + q) into centre slot pc.s, once the centre RC earlier is released.
             RingPos ps, pc;
-            int q = 0;
-            for (; q < NP; ++q) {
-                if (q >= R && !ptx::mbar_wait(&empty[ps.s], ps.ph ^ 1u, sp.err)) break;
-                const bool centre = NCEN > 0 && q >= 2 * G;
-                if (centre && q - 2 * G >= RC && !ptx::mbar_wait(&cempty[pc.s], pc.ph ^ 1u, sp.err)) break;
-                ptx::mbar_arrive_expect_tx(&full[ps.s], bytes + (centre ? cbytes : 0u));
-                // storage coordinates: x = x0 - XH + xoff (= x0), y = y0 - G + g (= y0), z = z0 - G + q + g
-                ptx::tma_load_4d(smem_raw + ps.s * SSLOT, &tmap, x0, y0, z0 + q, 0, &full[ps.s]);
-                if constexpr (NCEN > 0) {
-                    if (centre) {
-                        const int zc = z0 - 2 * G + q;
-                        unsigned char* cs = cring + pc.s * CSLOT;
-                        ptx::tma_load_4d(cs + RingT::C0_OFF, &cmaps.map[0], x0 + cmaps.x[0], y0 + cmaps.y[0],
-                                         zc + cmaps.z[0], 0, &full[ps.s]);
-                        if constexpr (NCEN > 1)
-                            ptx::tma_load_4d(cs + RingT::C1_OFF, &cmaps.map[1], x0 + cmaps.x[1], y0 + cmaps.y[1],
-                                             zc + cmaps.z[1], 0, &full[ps.s]);
-                        pc.next(RC);
-                    }
+            long long t = 0, tc = 0;
+            bool ok = true;
+            for (int m = 0; m < nitems && ok; ++m) {
+                const ItemBox b = src.item(m);
+                const CUtensorMap* tmap = src.stencil_map(b.inst);
+                const CentreMaps& cm = src.centre_maps(b.inst);
+                ptx::prefetch_tensor_map(tmap);
+                if constexpr (NCEN > 0) ptx::prefetch_tensor_map(&cm.map[0]);
+                if constexpr (NCEN > 1) ptx::prefetch_tensor_map(&cm.map[1]);
+                int cx[2] = {0, 0}, cy[2] = {0, 0}, cz[2] = {0, 0};
+#pragma unroll
+                for (int k = 0; k < NCEN; ++k) {
+                    cx[k] = cm.x[k];
+                    cy[k] = cm.y[k];
+                    cz[k] = cm.z[k];
                 }
-                ps.next(R);
+                const int NP = (b.z1 - b.z0) + 2 * G; // planes z0 - G .. z1 - 1 + G
+                for (int q = 0; q < NP; ++q, ++t) {
+                    if (t >= R && !ptx::mbar_wait(&empty[ps.s], ps.ph ^ 1u, err)) {
+                        ok = false;
+                        break;
+                    }
+                    const bool centre = NCEN > 0 && q >= 2 * G;
+                    if (centre && tc >= RC && !ptx::mbar_wait(&cempty[pc.s], pc.ph ^ 1u, err)) {
+                        ok = false;
+                        break;
+                    }
+                    ptx::mbar_arrive_expect_tx(&full[ps.s], bytes + (centre ? cbytes : 0u));
+                    // storage coordinates: x = x0 - XH + xoff (= x0), y = y0 - G + g (= y0), z = z0 - G + q + g
+                    ptx::tma_load_4d(smem_raw + ps.s * SSLOT, tmap, b.x0, b.y0, b.z0 + q, 0, &full[ps.s]);
+                    if constexpr (NCEN > 0) {
+                        if (centre) {
+                            const int zc = b.z0 - 2 * G + q;
+                            unsigned char* cs = cring + pc.s * CSLOT;
+                            ptx::tma_load_4d(cs + RingT::C0_OFF, &cm.map[0], b.x0 + cx[0], b.y0 + cy[0], zc + cz[0], 0,
+                                             &full[ps.s]);
+                            if constexpr (NCEN > 1)
+                                ptx::tma_load_4d(cs + RingT::C1_OFF, &cm.map[1], b.x0 + cx[1], b.y0 + cy[1],
+                                                 zc + cz[1], 0, &full[ps.s]);
+                            pc.next(RC);
+                            ++tc;
+                        }
+                    }
+                    ps.next(R);
+                }
             }
-            if (q < NP) {
+            if (!ok) {
                 // a consumer warp stopped releasing slots: let the copies in flight land
-                for (int r = (q > R ? q - R : 0); r < q; ++r)
+                for (long long r = (t > R ? t - R : 0); r < t; ++r)
                     ptx::mbar_wait(&full[r % R], uint32_t((r / R) & 1), nullptr, 100000000ull);
             }
         }
@@ -281,154 +364,180 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
     if (warp > TY) return;
 
     // -------------------------------------------------------------------- consumer warps
-    // Register copies of everything the plane loop reads: values in kernel-parameter space are
-    // not known to be loop-invariant, which would keep e.g. the stencils' 1/dx factors and the
-    // functor's data inside the loop.
-    const RHS f = rhs;
-    const amrex::GeometryData geom = sp.geom;
-    const Layout L = sp.L;
-    const double time = sp.time;
-    const typename Epi::Params epl = ep;
-
     constexpr int CX = Cfg::CX, U = Cfg::U;
     constexpr int QL = 2 * G + U; // register queue depth (planes)
     const int tx = lane, ty = warp;
-    const int i0 = x0 + CX * tx, j = y0 + ty; // this thread's cells: (i0 + e, j), e < CX
-    bool act[CX];
-#pragma unroll
-    for (int e = 0; e < CX; ++e) act[e] = (i0 + e < L.n[0]) && (j < L.n[1]);
     const int coff = (ty + G) * BX + (CX * tx + XH); // cell 0's centre inside the stencil plane
     const int cc = ty * TX + CX * tx;                // ... inside a centre-operand box
 
-    // q[e][m * NC + c]: column of cell e, plane it - 2G - U + m (before the shift of iteration it)
-    T q[CX][QL * NC];
-#pragma unroll
-    for (int e = 0; e < CX; ++e)
-#pragma unroll
-        for (int m = 0; m < QL * NC; ++m) q[e][m] = T(0);
-
-    const T* in_col = sp.in + L.index(i0, j, 0, 0); // global fallback: cell 0's column at z = 0
-    const long long plane = L.px * L.py;
-
-    // Prologue: planes 0 .. 2G-1 (the chunk's lower halo and first G centre planes) into the
-    // queue; planes below the chunk (p < G) are released at once.
-    RingPos pos; // plane it
+    RingPos pos;  // stencil slot of the item's plane it
+    RingPos kpos; // centre slot of the item's centre plane it - G
     bool ok = true;
-#pragma unroll
-    for (int p = 0; p < 2 * G; ++p) {
-        if (ok && !ptx::mbar_wait(&full[pos.s], pos.ph, sp.err)) ok = false;
-        if (ok) {
-            const T* pl = reinterpret_cast<const T*>(smem_raw + pos.s * SSLOT) + coff;
-#pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                T v[CX];
-                lds<CX>(pl + c * PNS, v);
-#pragma unroll
-                for (int e = 0; e < CX; ++e) q[e][(p + U) * NC + c] = v[e];
-            }
-            if (p < G) {
-                __syncwarp();
-                if (lane == 0) ptx::mbar_arrive(&empty[pos.s]);
-            }
-        }
-        pos.next(R);
-    }
-    if (!ok) return;
+    for (int m = 0; m < nitems && ok; ++m) {
+        const ItemBox b = src.item(m);
+        // Register copies of everything the plane loop reads: values in kernel-parameter or
+        // global space are not known to be loop-invariant, which would keep e.g. the
+        // stencils' 1/dx factors and the functor's data inside the loop.
+        const RHS f = src.rhs_of(b.inst);
+        const StageParams<T>& spr = src.params(b.inst);
+        const amrex::GeometryData geom = spr.geom;
+        const Layout L = spr.L;
+        const double time = spr.time;
+        const T* const in = spr.in;
+        const typename Epi::Params epl = src.epi(b.inst);
 
-    // Main loop: U planes per iteration. Cell (e, u) has centre plane it - G + u, i.e.
-    // z = z0 - 2G + it + u, and exists while it + u < NP; its queue window is q[e][u ...] and
-    // its centre operands are centre slot number it - 2G + u. After the iteration its centre
-    // plane and centre slot are released; the last G stencil planes need no release, since no
-    // copy waits for their slots.
-    RingPos cpos; // stencil slot of plane it - G
-    cpos.s = G;
-    RingPos kpos; // centre slot of centre plane it - G
-    for (int it = 2 * G; it < NP; it += U) {
-        int su[U], scu[U], sku[U];
-        {
-            RingPos pp = pos, cp = cpos, kp = kpos;
+        const int NP = (b.z1 - b.z0) + 2 * G;
+        const int i0 = b.x0 + CX * tx, j = b.y0 + ty; // this thread's cells: (i0 + e, j), e < CX
+        bool act[CX];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                su[u] = pp.s;
-                scu[u] = cp.s;
-                sku[u] = kp.s;
-                if (it + u < NP && !ptx::mbar_wait(&full[pp.s], pp.ph, sp.err)) ok = false;
-                pp.next(R);
-                cp.next(R);
-                if constexpr (NCEN > 0) kp.next(RC);
-            }
-        }
-        if (!ok) break;
+        for (int e = 0; e < CX; ++e) act[e] = (i0 + e < L.n[0]) && (j < L.n[1]);
+
+        // q[e][m * NC + c]: column of cell e, plane it - 2G - U + m (before the shift of iteration it)
+        T q[CX][QL * NC];
 #pragma unroll
         for (int e = 0; e < CX; ++e)
 #pragma unroll
-            for (int m = 0; m < 2 * G * NC; ++m) q[e][m] = q[e][m + U * NC];
+            for (int mm = 0; mm < QL * NC; ++mm) q[e][mm] = T(0);
+
+        const T* in_col = in + L.index(i0, j, 0, 0); // global fallback: cell 0's column at z = 0
+        const long long plane = L.px * L.py;
+
+        // Prologue: planes 0 .. 2G-1 (the lower halo and the first G centre planes) into the
+        // queue. Planes that are never centre planes (p < G, p >= NP - G) are released once
+        // read; every other plane after its iteration as a centre plane.
+        RingPos cpos; // stencil slot of plane it - G
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            if (U == 1 || it + u < NP) {
-                const T* pl = reinterpret_cast<const T*>(smem_raw + su[u] * SSLOT) + coff;
+        for (int p = 0; p < 2 * G; ++p) {
+            if (p == G) cpos = pos;
+            if (ok && !ptx::mbar_wait(&full[pos.s], pos.ph, err)) ok = false;
+            if (ok) {
+                const T* pl = reinterpret_cast<const T*>(smem_raw + pos.s * SSLOT) + coff;
 #pragma unroll
                 for (int c = 0; c < NC; ++c) {
                     T v[CX];
                     lds<CX>(pl + c * PNS, v);
 #pragma unroll
-                    for (int e = 0; e < CX; ++e) q[e][(2 * G + u) * NC + c] = v[e];
+                    for (int e = 0; e < CX; ++e) q[e][(p + U) * NC + c] = v[e];
+                }
+                if (p < G || p >= NP - G) {
+                    __syncwarp();
+                    if (lane == 0) ptx::mbar_arrive(&empty[pos.s]);
                 }
             }
-        }
-
-        // all cells' stage values first, then the epilogues (their global stores would
-        // otherwise stand between the shared-memory taps of neighbouring cells)
-        T kv[U][CX][NC];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int z = z0 - 2 * G + it + u;
-            const T* ctr = reinterpret_cast<const T*>(smem_raw + scu[u] * SSLOT) + coff;
-#pragma unroll
-            for (int e = 0; e < CX; ++e) {
-#pragma unroll
-                for (int c = 0; c < NC; ++c) kv[u][e][c] = T(0);
-                if ((U == 1 || it + u < NP) && act[e]) {
-                    amrex::StencilView<T> view{ctr + e,       q[e] + u * NC, in_col + e + z * plane, L.px, plane,
-                                               L.comp_stride(), i0 + e,      j, z, BX, PNS, G, NC};
-                    amrex::Array4<const T> arr = make_array4<const T>(sp.in, L);
-                    arr.view = &view;
-                    typename RHS::Workspace ws{};
-                    const amrex::IntVect idx{i0 + e, j, z};
-                    treesap::static_for<NC>([&]<int c>() {
-                        kv[u][e][c] = static_cast<T>(f.template operator()<c>(idx, time, arr, geom, ws));
-                    });
-                }
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            if (U == 1 || it + u < NP) {
-                const int z = z0 - 2 * G + it + u;
-                const unsigned char* cslot = cring + sku[u] * CSLOT;
-                const CentreOps<C0, C1> co{reinterpret_cast<const C0*>(cslot + RingT::C0_OFF) + cc,
-                                           reinterpret_cast<const C1*>(cslot + RingT::C1_OFF) + cc, CPS};
-                Epi::template apply<T, NC, CX>(epl, kv[u], act,
-                                               reinterpret_cast<const T*>(smem_raw + scu[u] * SSLOT) + coff, PNS,
-                                               i0, j, z, co);
-            }
-        }
-        __syncwarp();
-        if (lane == 0) {
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (U == 1 || it + u < NP) {
-                    ptx::mbar_arrive(&empty[scu[u]]);
-                    if constexpr (NCEN > 0) ptx::mbar_arrive(&cempty[sku[u]]);
-                }
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
             pos.next(R);
-            cpos.next(R);
-            if constexpr (NCEN > 0) kpos.next(RC);
+        }
+        if (!ok) break;
+
+        // Main loop: U planes per iteration. Cell (e, u) has centre plane it - G + u, i.e.
+        // z = z0 - 2G + it + u, and exists while it + u < NP; its queue window is q[e][u ...].
+        for (int it = 2 * G; it < NP; it += U) {
+            int su[U], scu[U], sku[U];
+            {
+                RingPos pp = pos, cp = cpos, kp = kpos;
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    su[u] = pp.s;
+                    scu[u] = cp.s;
+                    sku[u] = kp.s;
+                    if (it + u < NP && !ptx::mbar_wait(&full[pp.s], pp.ph, err)) ok = false;
+                    pp.next(R);
+                    cp.next(R);
+                    if constexpr (NCEN > 0) kp.next(RC);
+                }
+            }
+            if (!ok) break;
+#pragma unroll
+            for (int e = 0; e < CX; ++e)
+#pragma unroll
+                for (int mm = 0; mm < 2 * G * NC; ++mm) q[e][mm] = q[e][mm + U * NC];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (U == 1 || it + u < NP) {
+                    const T* pl = reinterpret_cast<const T*>(smem_raw + su[u] * SSLOT) + coff;
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        T v[CX];
+                        lds<CX>(pl + c * PNS, v);
+#pragma unroll
+                        for (int e = 0; e < CX; ++e) q[e][(2 * G + u) * NC + c] = v[e];
+                    }
+                }
+            }
+
+            // all cells' stage values first, then the epilogues (their global stores would
+            // otherwise stand between the shared-memory taps of neighbouring cells)
+            T kv[U][CX][NC];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int z = b.z0 - 2 * G + it + u;
+                const T* ctr = reinterpret_cast<const T*>(smem_raw + scu[u] * SSLOT) + coff;
+#pragma unroll
+                for (int e = 0; e < CX; ++e) {
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) kv[u][e][c] = T(0);
+                    if ((U == 1 || it + u < NP) && act[e]) {
+                        amrex::StencilView<T> view{ctr + e,         q[e] + u * NC, in_col + e + z * plane, L.px, plane,
+                                                   L.comp_stride(), i0 + e,        j, z, BX, PNS, G, NC};
+                        amrex::Array4<const T> arr = make_array4<const T>(in, L);
+                        arr.view = &view;
+                        typename RHS::Workspace ws{};
+                        const amrex::IntVect idx{i0 + e, j, z};
+                        treesap::static_for<NC>([&]<int c>() {
+                            kv[u][e][c] = static_cast<T>(f.template operator()<c>(idx, time, arr, geom, ws));
+                        });
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (U == 1 || it + u < NP) {
+                    const int z = b.z0 - 2 * G + it + u;
+                    const unsigned char* cslot = cring + sku[u] * CSLOT;
+                    const CentreOps<C0, C1> co{reinterpret_cast<const C0*>(cslot + RingT::C0_OFF) + cc,
+                                               reinterpret_cast<const C1*>(cslot + RingT::C1_OFF) + cc, CPS};
+                    Epi::template apply<T, NC, CX>(epl, kv[u], act,
+                                                   reinterpret_cast<const T*>(smem_raw + scu[u] * SSLOT) + coff,
+                                                   PNS, i0, j, z, co);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) {
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (U == 1 || it + u < NP) {
+                        ptx::mbar_arrive(&empty[scu[u]]);
+                        if constexpr (NCEN > 0) ptx::mbar_arrive(&cempty[sku[u]]);
+                        if (it + u >= NP - G) ptx::mbar_arrive(&empty[su[u]]);
+                    }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (U == 1 || it + u < NP) {
+                    pos.next(R);
+                    cpos.next(R);
+                    if constexpr (NCEN > 0) kpos.next(RC);
+                }
+            }
         }
     }
+}
+
+template <class Cfg, class RHS, class Epi>
+__global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
+    stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CentreMaps cmaps,
+                 const __grid_constant__ StageParams<typename Cfg::T> sp, const __grid_constant__ RHS rhs,
+                 const __grid_constant__ typename Epi::Params ep) {
+    const SingleSource<Cfg, RHS, Epi> src{&tmap, &cmaps, &sp, &rhs, &ep};
+    stage_body<Cfg, RHS, Epi>(src);
+}
+
+/// Persistent batched form: one launch for all items of all instances.
+template <class Cfg, class RHS, class Epi>
+__global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
+    batch_stage_kernel(const StageEntry<Cfg, RHS, Epi>* __restrict__ entries, const ItemBox* __restrict__ items,
+                       int nitems, int ty, int* err) {
+    const BatchSource<Cfg, RHS, Epi> src{entries, items, nitems, ty, err};
+    stage_body<Cfg, RHS, Epi>(src);
 }
 
 // ------------------------------------------------------------------ epilogues
