@@ -15,6 +15,8 @@ Timing: K steps bracketed by barrier + synchronize, CUDA events on the library's
 max over ranks. Every field (268 MB) is larger than L2 (126 MB), so no L2 flush is needed
 between steps. `e2e` times the C ABI call ts_integrator_run (pinned host state in -> 20
 steps -> host state out) with the host<->device copies inside the timed region.
+The line also carries `batched`: the C4 workload (512 periodic instances, edges 16..96) through
+ts_batch_* (autotuned launch shape, one persistent launch per stage, CUDA graph), 200 steps.
 For N > 1 every rank runs an independent replica (weak scaling; the z-slab halo exchange of
 a sharded domain is not part of this build).
 """
@@ -39,6 +41,7 @@ METRIC = "RK4 cell-updates/s @256^3: FP32 vs FP64 at err<=1e-6; % of HBM peak"
 UNIT = "cell-updates/s"
 N = 256
 E2E_CHUNK = 20  # steps per end-to-end call (the plot-export cadence of the reference's driver)
+BATCH_STEPS = 200  # C4 step count
 # Algorithmic HBM bytes per cell and launch (2 components, valid cells only, ghost fills excluded).
 ALG_BYTES = {
     # FP32-stage per component: R u8 W k0 8 W u_p 8 | R k0 8 W d1 4 | R d1 4 W d2 4 | R d2 4, d1 4, u_p 8 W u 8
@@ -317,6 +320,26 @@ def run_b200(args, rank, world, local_rank):
 
     cpu = cpu_baseline(c2_desc(TS_F64, N), pulses) if (rank == 0 and world == 1) else None
 
+    # batched form (C4): 512 periodic instances, one persistent launch per stage, CUDA graph
+    batched = None
+    for r in res.values():
+        r["it"].close()  # free the 256^3 fields first
+    try:
+        from treesap_b200.run_batch import run as run_batch
+
+        dist.barrier()
+        b = run_batch(ctx, steps=BATCH_STEPS, warmup=3, form="f32", autotune=True, graph=True)
+        ms_b = dist.max(b["ms"])
+        vb = world * b["cells"] * BATCH_STEPS / (ms_b * 1e-3)
+        batched = {"workload": "C4: 512 periodic scalar-wave instances, edges U{16,24,...,96}, ngrow 2, no KO, "
+                               "RK4 dt=0.25/n, one Gaussian each, FP32-stage", "value": vb, "unit": UNIT,
+                   "steps": BATCH_STEPS, "ms_per_step": ms_b / BATCH_STEPS, "cells": b["cells"],
+                   "launches_per_step": b["launches"] / BATCH_STEPS, "launch_shape_rows_zchunk": list(b["shape"]),
+                   "hbm_frac_of_step": sum(ALG_BYTES["f32"].values()) * vb / world / 1e9 / peak}
+        b["batch"].close()
+    except Exception as ex:  # noqa: BLE001 - reported in the line
+        batched = {"value": None, "error": str(ex)}
+
     if rank == 0:
         f32, f64 = res["f32"], res["f64"]
         line = {
@@ -341,10 +364,9 @@ def run_b200(args, rank, world, local_rank):
             "gpu_launches": int(f32["launches"]),
             "clocks": {k: f32["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
             "clocks_fp64_run": {k: f64["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+            "batched": batched,
         }
         print(json.dumps(line))
-    for r in res.values():
-        r["it"].close()
     ctx.close()
     dist.close()
 

@@ -6,12 +6,18 @@
       profile s^2, max strength 10/L, targets 0 (Dirichlet-0 ghosts), RK4 dt = 0.25 dx,
       1000 steps; phi0 = sum of 8 Gaussians, A ~ U[0.5, 1], w ~ U[0.05, 0.15],
       c ~ U[0.25, 0.75]^3, pi0 = 0; FP64 and FP32-stage.
+  C4  512 independent instances, cube edges n ~ U{16, 24, ..., 96}, unit cube (dx = 1/n),
+      periodic, 4th-order stencils (ngrow 2), no KO, RK4 dt = 0.25/n each, 200 steps;
+      one Gaussian per instance, A ~ U[0.5, 1], w ~ U[0.05, 0.2], c ~ U[0.3, 0.7]^3;
+      FP32-stage, one persistent launch per stage, CUDA graph.
 """
 from __future__ import annotations
 
 import numpy as np
 
-from . import TS_BC_DIRICHLET, TS_BC_NOOP, TS_F64, TS_MODEL_WAVE, TS_RK4, WaveDesc
+from . import TS_BC_DIRICHLET, TS_BC_NOOP, TS_F32_STAGE, TS_F64, TS_MODEL_WAVE, TS_RK4, WaveDesc
+
+TS_F32_STAGE_DEFAULT = TS_F32_STAGE
 
 
 def wave_desc(
@@ -91,3 +97,22 @@ def c2_pulses(seed: int = 2024, npulses: int = 8) -> np.ndarray:
 
 C1_STEPS = 100
 C2_STEPS = 1000
+
+
+C4_STEPS = 200
+
+
+def c4_descs(precision: int = TS_F32_STAGE_DEFAULT, count: int = 512, seed: int = 4004) -> list[WaveDesc]:
+    rng = np.random.default_rng(seed)
+    edges = rng.choice(np.arange(16, 97, 8), size=count)
+    return [wave_desc(int(n), 2, periodic=(1, 1, 1), precision=precision, dt=0.25 / int(n)) for n in edges]
+
+
+def c4_pulses(count: int = 512, seed: int = 4005) -> list[np.ndarray]:
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        a, w = rng.uniform(0.5, 1.0), rng.uniform(0.05, 0.2)
+        c = rng.uniform(0.3, 0.7, 3)
+        out.append(np.array([[0, a, w, *c]], dtype=np.float64))
+    return out
