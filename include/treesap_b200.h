@@ -196,6 +196,32 @@ TS_API ts_status ts_batch_autotune(ts_batch* b, int trial_steps, int* rows, int*
 /* Device time and kernel launches of the last ts_batch_step call (valid after ts_context_sync). */
 TS_API ts_status ts_batch_last_step_timing(ts_batch* b, double* ms, long long* launches);
 
+/* ------------------------------------------------------------------ discrete adjoint
+ * No counterpart in the reference. Variable-speed scalar wave model
+ *   phi_t = pi + s K phi,   pi_t = c(x)^2 sum_a D2_aa phi + s K pi
+ * (D2 centred of half-width ngrow, K the Kreiss-Oliger operator of order ngrow, s =
+ * ko_strength) on a periodic grid, RK4 in FP64: the same arithmetic as ts_integrator_* with
+ * KO and a c2 field. desc: TS_MODEL_WAVE, ngrow 2 or 4, periodic in every direction,
+ * TS_RK4, TS_PRECISION_F64, no absorbing layer; desc->c2 is ignored (the speed is an argument
+ * of every call). All arrays are host arrays of the valid cells (x fastest, n0 n1 n2 values).
+ * Loss J = 1/2 sum_cells (phi(T) - phi_target)^2. The reverse sweep runs RK4 with the
+ * transposed operator, recomputing the forward states from checkpoints taken every
+ * `checkpoint_every` steps. */
+typedef struct ts_adjoint ts_adjoint;
+TS_API ts_status ts_adjoint_create(ts_context* ctx, const ts_wave_desc* desc, int checkpoint_every, ts_adjoint** out);
+TS_API ts_status ts_adjoint_destroy(ts_adjoint* a);
+/* phi(T), pi(T) after nsteps from (phi0, pi0 (NULL = 0)) with speed c; outputs may be NULL. */
+TS_API ts_status ts_adjoint_forward(ts_adjoint* a, const double* phi0, const double* pi0, const double* c, int nsteps,
+                                    double* phi_T, double* pi_T);
+/* J and dJ/dphi0, dJ/dpi0, dJ/dc (any output may be NULL). */
+TS_API ts_status ts_adjoint_gradient(ts_adjoint* a, const double* phi0, const double* pi0, const double* c, int nsteps,
+                                     const double* phi_target, double* loss, double* grad_phi0, double* grad_pi0,
+                                     double* grad_c);
+/* Tangent-linear run: the perturbation (dphi(T), dpi(T)) caused by (dphi0, dpi0, dc) (NULL = 0). */
+TS_API ts_status ts_adjoint_tangent(ts_adjoint* a, const double* phi0, const double* pi0, const double* c,
+                                    const double* dphi0, const double* dpi0, const double* dc, int nsteps,
+                                    double* dphi_T, double* dpi_T);
+
 /* ------------------------------------------------------------------ allocation-free stepping
  * No counterpart in the reference. For callers that must not allocate device memory: host
  * applications that own all device memory through their own pool or arena, and loops that

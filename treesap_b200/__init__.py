@@ -22,6 +22,7 @@ __all__ = [
     "Context",
     "Integrator",
     "Batch",
+    "Adjoint",
     "TS_EULER",
     "TS_RK4",
     "TS_F64",
@@ -155,6 +156,11 @@ def lib() -> C.CDLL:
         "ts_batch_set_launch_shape": (i, [vp, i, i]),
         "ts_batch_autotune": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
         "ts_batch_last_step_timing": (i, [vp, C.POINTER(d), C.POINTER(ll)]),
+        "ts_adjoint_create": (i, [vp, C.POINTER(WaveDesc), i, C.POINTER(vp)]),
+        "ts_adjoint_destroy": (i, [vp]),
+        "ts_adjoint_forward": (i, [vp, vp, vp, vp, i, vp, vp]),
+        "ts_adjoint_gradient": (i, [vp, vp, vp, vp, i, vp, C.POINTER(d), vp, vp, vp]),
+        "ts_adjoint_tangent": (i, [vp, vp, vp, vp, vp, vp, vp, i, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -350,6 +356,67 @@ class Batch:
     def close(self) -> None:
         if self.handle:
             lib().ts_batch_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _ptr(a: np.ndarray | None) -> int | None:
+    return None if a is None else a.ctypes.data
+
+
+class Adjoint:
+    """Discrete adjoint and tangent-linear model of the variable-speed wave system (ts_adjoint).
+
+    Arrays are (nz, ny, nx) float64 host arrays of the valid cells; c is the wave speed.
+    """
+
+    def __init__(self, ctx: Context, desc: WaveDesc, checkpoint_every: int = 20):
+        self.ctx = ctx
+        self.shape = (desc.n[2], desc.n[1], desc.n[0])
+        self.handle = C.c_void_p()
+        _check(lib().ts_adjoint_create(ctx.handle, C.byref(desc), checkpoint_every, C.byref(self.handle)),
+               "ts_adjoint_create", ctx)
+        ctx._adopt(self)
+
+    def _in(self, a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        assert a.shape == self.shape, (a.shape, self.shape)
+        return a
+
+    def forward(self, phi0, pi0, c, nsteps: int):
+        phi0, pi0, c = self._in(phi0), self._in(pi0), self._in(c)
+        phi, pi = np.empty(self.shape), np.empty(self.shape)
+        _check(lib().ts_adjoint_forward(self.handle, _ptr(phi0), _ptr(pi0), _ptr(c), nsteps, _ptr(phi), _ptr(pi)),
+               "ts_adjoint_forward", self.ctx)
+        return phi, pi
+
+    def gradient(self, phi0, pi0, c, nsteps: int, target):
+        """(J, dJ/dphi0, dJ/dpi0, dJ/dc) for J = 1/2 sum (phi(T) - target)^2."""
+        phi0, pi0, c, target = self._in(phi0), self._in(pi0), self._in(c), self._in(target)
+        gphi, gpi, gc = np.empty(self.shape), np.empty(self.shape), np.empty(self.shape)
+        loss = C.c_double()
+        _check(lib().ts_adjoint_gradient(self.handle, _ptr(phi0), _ptr(pi0), _ptr(c), nsteps, _ptr(target),
+                                         C.byref(loss), _ptr(gphi), _ptr(gpi), _ptr(gc)),
+               "ts_adjoint_gradient", self.ctx)
+        return loss.value, gphi, gpi, gc
+
+    def tangent(self, phi0, pi0, c, dphi0, dpi0, dc, nsteps: int):
+        args = [self._in(a) for a in (phi0, pi0, c, dphi0, dpi0, dc)]
+        dphi, dpi = np.empty(self.shape), np.empty(self.shape)
+        _check(lib().ts_adjoint_tangent(self.handle, *[_ptr(a) for a in args], nsteps, _ptr(dphi), _ptr(dpi)),
+               "ts_adjoint_tangent", self.ctx)
+        return dphi, dpi
+
+    def close(self) -> None:
+        if self.handle:
+            lib().ts_adjoint_destroy(self.handle)
             self.handle = C.c_void_p()
 
     def __del__(self):

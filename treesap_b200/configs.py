@@ -116,3 +116,36 @@ def c4_pulses(count: int = 512, seed: int = 4005) -> list[np.ndarray]:
         c = rng.uniform(0.3, 0.7, 3)
         out.append(np.array([[0, a, w, *c]], dtype=np.float64))
     return out
+
+
+C5_STEPS = 200
+C5_CHECKPOINT_EVERY = 20
+
+
+def c5_desc(n: int = 128, ngrow: int = 2) -> WaveDesc:
+    """C5: 128^3 periodic unit cube, phi_t = pi, pi_t = c(x)^2 sum D2 phi + KO 0.1 (order ngrow), RK4 dt = 0.25 dx."""
+    return wave_desc(n, ngrow, periodic=(1, 1, 1), ko=0.1)
+
+
+def c5_speed(n: int = 128, seed: int = 5005, modes: int = 16, kmax: int = 4) -> np.ndarray:
+    """c = 1 + 0.2 f / max|f|, f a sum of `modes` seeded Fourier modes with |k| <= kmax; (nz, ny, nx)."""
+    rng = np.random.default_rng(seed)
+    x = (np.arange(n) + 0.5) / n
+    z3, y3, x3 = np.meshgrid(x, x, x, indexing="ij")
+    f = np.zeros((n, n, n))
+    added = 0
+    while added < modes:
+        k = rng.integers(-kmax, kmax + 1, 3)
+        if not k.any() or np.linalg.norm(k) > kmax:
+            continue
+        f += rng.normal() * np.cos(2 * np.pi * (k[0] * x3 + k[1] * y3 + k[2] * z3) + rng.uniform(0, 2 * np.pi))
+        added += 1
+    return 1.0 + 0.2 * f / np.abs(f).max()
+
+
+def c5_pulse(n: int = 128, shift_cells: float = 0.0, amplitude: float = 1.0, width: float = 0.1) -> np.ndarray:
+    """phi0 = A exp(-|x - c|^2 / w^2), c = (1/2 + shift dx, 1/2, 1/2); (nz, ny, nx)."""
+    x = (np.arange(n) + 0.5) / n
+    z3, y3, x3 = np.meshgrid(x, x, x, indexing="ij")
+    cx = 0.5 + shift_cells / n
+    return amplitude * np.exp(-((x3 - cx) ** 2 + (y3 - 0.5) ** 2 + (z3 - 0.5) ** 2) / width**2)
