@@ -16,7 +16,9 @@ max over ranks. Every field (268 MB) is larger than L2 (126 MB), so no L2 flush 
 between steps. `e2e` times the C ABI call ts_integrator_run (pinned host state in -> 20
 steps -> host state out) with the host<->device copies inside the timed region.
 The line also carries `batched`: the C4 workload (512 periodic instances, edges 16..96) through
-ts_batch_* (autotuned launch shape, one persistent launch per stage, CUDA graph), 200 steps.
+ts_batch_* (autotuned launch shape, one persistent launch per stage, CUDA graph), 200 steps, and
+`adjoint`: the C5 loss + gradient through ts_adjoint_* (seconds, and the largest relative
+difference to central finite differences over 32 random directions of phi0 and of c).
 For N > 1 every rank runs an independent replica (weak scaling; the z-slab halo exchange of
 a sharded domain is not part of this build).
 """
@@ -340,6 +342,21 @@ def run_b200(args, rank, world, local_rank):
     except Exception as ex:  # noqa: BLE001 - reported in the line
         batched = {"value": None, "error": str(ex)}
 
+    # discrete adjoint (C5): loss + gradient time and central-difference agreement
+    adjoint = None
+    try:
+        from treesap_b200.run_adjoint import run as run_adjoint
+
+        a = run_adjoint(ctx)
+        adjoint = {"workload": "C5: 128^3 periodic variable-speed wave, ngrow 2, KO 0.1, RK4 200 steps, checkpoints "
+                               "every 20, J = 1/2 sum (phi(T) - phi_target)^2, FP64",
+                   "gradient_seconds": a["gradient_s"], "forward_seconds": a["forward_s"],
+                   "gradient_over_forward": a["gradient_s"] / a["forward_s"],
+                   "fd_directions": a["directions"], "fd_rel_err_max_phi0": a["fd_rel_max_phi0"],
+                   "fd_rel_err_max_c": a["fd_rel_max_c"], "tolerance": 1e-5}
+    except Exception as ex:  # noqa: BLE001 - reported in the line
+        adjoint = {"error": str(ex)}
+
     if rank == 0:
         f32, f64 = res["f32"], res["f64"]
         line = {
@@ -365,6 +382,7 @@ def run_b200(args, rank, world, local_rank):
             "clocks": {k: f32["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
             "clocks_fp64_run": {k: f64["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
             "batched": batched,
+            "adjoint": adjoint,
         }
         print(json.dumps(line))
     ctx.close()
