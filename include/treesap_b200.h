@@ -48,7 +48,12 @@ typedef enum ts_precision {
     TS_PRECISION_F64 = 0,      /* plain form: FP64 throughout, the reference's register scheme */
     TS_PRECISION_F32_STAGE = 1 /* FP32 stage arithmetic and storage, FP64 state and final combination */
 } ts_precision;
-typedef enum ts_init_kind { TS_INIT_STATE = 0, TS_INIT_GAUSSIAN = 1, TS_INIT_FOURIER = 2 } ts_init_kind;
+typedef enum ts_init_kind {
+    TS_INIT_STATE = 0,
+    TS_INIT_GAUSSIAN = 1,
+    TS_INIT_FOURIER = 2,
+    TS_INIT_EXPRESSION = 3 /* ts_integrator_initialise_expressions */
+} ts_init_kind;
 
 /* ------------------------------------------------------------------ runtime */
 typedef struct ts_context ts_context;
@@ -129,6 +134,19 @@ TS_API int ts_integrator_ncomp(const ts_integrator* it);
  * TS_INIT_GAUSSIAN: nitems pulses {comp, A, w, cx, cy, cz};
  * TS_INIT_FOURIER: nitems modes {comp, A, kx, ky, kz, phase}. Resets time and step count. */
 TS_API ts_status ts_integrator_initialise(ts_integrator* it, int init_kind, int nitems, const double* items);
+
+/* initialise() with treesap::FunctionInit (init/FunctionInit.hpp:34-101): one expression of
+ * x, y, z per component (count = ncomp), e.g. "exp(-(x^2 + y^2 + z^2)/0.1^2)", compiled on the
+ * host and evaluated at the cell centres on the device. Operators + - * / ^ ** (right
+ * associative), comparisons, and / or, functions sin cos tan asin acos atan sinh cosh tanh exp
+ * log log10 sqrt abs floor ceil erf heaviside pow atan2 min max fmod if(c, a, b), constant pi.
+ * Invalid text returns TS_ERR_INVALID_ARGUMENT (message in ts_context_last_error). */
+TS_API ts_status ts_integrator_initialise_expressions(ts_integrator* it, int count, const char* const* exprs);
+
+/* Host evaluation of one expression at n points (the program the device evaluates); for
+ * checking expressions without a device. */
+TS_API ts_status ts_expression_eval(const char* expr, int n, const double* x, const double* y, const double* z,
+                                    double* out);
 
 /* Valid-cell state, component-major [comp][z][y][x] FP64. `src`/`dst` are host pointers
  * (pageable or pinned) unless *_is_device is nonzero. set_state resets time and step count. */

@@ -175,3 +175,19 @@ def test_static_ghost_fills_run_once_per_buffer(ctx, port_oracle, precision):
     it_p.step(1)
     ctx.sync()
     assert it_p.last_step_timing()[1] == 8
+
+
+def test_function_init_expressions_match_numpy(ctx):
+    """FunctionInit through the C ABI: device evaluation of the compiled expressions at cell centres."""
+    n = (20, 24, 28)
+    lo, hi = (-2.0, -1.0, 0.0), (2.0, 1.0, 1.5)
+    d = wave_desc(n, 2, periodic=(0, 0, 0), prob_lo=lo, prob_hi=hi, bc=TS_BC_DIRICHLET)
+    it = Integrator(ctx, d)
+    it.initialise_expressions(["exp(-(x^2 + y^2 + z^2)/0.5^2)", "sin(pi*x)*y + z^3 - if(x < 0, 1, 0)"])
+    got = it.get_state()
+    c = [lo[a] + (np.arange(n[a]) + 0.5) * (hi[a] - lo[a]) / n[a] for a in range(3)]
+    z, y, x = np.meshgrid(c[2], c[1], c[0], indexing="ij")
+    want = np.stack([np.exp(-(x**2 + y**2 + z**2) / 0.5**2), np.sin(np.pi * x) * y + z**3 - (x < 0)])
+    np.testing.assert_allclose(got, want, rtol=1e-14, atol=1e-15)
+    with pytest.raises(Exception):
+        it.initialise_expressions(["exp(", "0"])

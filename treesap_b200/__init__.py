@@ -41,7 +41,7 @@ TS_OK = 0
 TS_EULER, TS_RK4 = 0, 1
 TS_F64, TS_F32_STAGE = 0, 1
 TS_BC_NOOP, TS_BC_DIRICHLET = 0, 1
-TS_INIT_STATE, TS_INIT_GAUSSIAN, TS_INIT_FOURIER = 0, 1, 2
+TS_INIT_STATE, TS_INIT_GAUSSIAN, TS_INIT_FOURIER, TS_INIT_EXPRESSION = 0, 1, 2, 3
 TS_MODEL_WAVE, TS_MODEL_TENSOR_WAVE = 0, 1
 STATUS_NAMES = {
     0: "TS_OK",
@@ -145,6 +145,8 @@ def lib() -> C.CDLL:
         "ts_integrator_last_step_timing": (i, [vp, C.POINTER(d), C.POINTER(ll)]),
         "ts_integrator_profile": (i, [vp, i, i, C.POINTER(ll), C.POINTER(d)]),
         "ts_integrator_set_launch_shape": (i, [vp, i, i]),
+        "ts_integrator_initialise_expressions": (i, [vp, i, vp]),
+        "ts_expression_eval": (i, [C.c_char_p, i, vp, vp, vp, vp]),
         "ts_batch_create": (i, [vp, vp, i, C.POINTER(vp)]),
         "ts_batch_destroy": (i, [vp]),
         "ts_batch_size": (i, [vp]),
@@ -236,6 +238,12 @@ class Integrator:
             "ts_integrator_initialise",
             self.ctx,
         )
+
+    def initialise_expressions(self, exprs: list[str]) -> None:
+        """FunctionInit: one expression of x, y, z per component."""
+        arr = (C.c_char_p * len(exprs))(*[e.encode() for e in exprs])
+        _check(lib().ts_integrator_initialise_expressions(self.handle, len(exprs), C.cast(arr, C.c_void_p)),
+               "ts_integrator_initialise_expressions", self.ctx)
 
     def set_state(self, state: np.ndarray) -> None:
         a = np.ascontiguousarray(state, dtype=np.float64)
@@ -424,3 +432,13 @@ class Adjoint:
             self.close()
         except Exception:
             pass
+
+
+def expression_eval(expr: str, x, y, z) -> np.ndarray:
+    """Host evaluation of an initial-condition expression (the program the device runs)."""
+    x, y, z = (np.ascontiguousarray(np.broadcast_to(a, np.broadcast(x, y, z).shape), dtype=np.float64)
+               for a in (x, y, z))
+    out = np.empty(x.shape)
+    _check(lib().ts_expression_eval(expr.encode(), x.size, x.ctypes.data, y.ctypes.data, z.ctypes.data,
+                                    out.ctypes.data), f"ts_expression_eval({expr!r})")
+    return out

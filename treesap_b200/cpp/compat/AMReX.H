@@ -289,8 +289,7 @@ class BCRec {
 };
 
 // ------------------------------------------------------------------ runtime stubs
-inline void Initialize(int&, char**&) {}
-inline void Initialize(int, char**) {}
+inline void Initialize(int&, char**&, bool = true) {}
 inline void Finalize() {}
 
 struct PrintStream {

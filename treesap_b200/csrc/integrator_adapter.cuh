@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstring>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -19,6 +20,7 @@
 #include "pde-model/bcs/DirichletBC.hpp"
 #include "pde-model/bcs/NoOpBC.hpp"
 #include "pde-model/rhs-decorators/KODecorator.hpp"
+#include "util/expression.hpp"
 
 #include "InitFunctors.hpp"
 #include "TensorWaveRHS.hpp"
@@ -28,7 +30,10 @@ namespace treesap_b200 {
 
 /// Initial condition read from a device parameter table:
 ///   table[0] = kind (TS_INIT_GAUSSIAN / TS_INIT_FOURIER), table[1] = count, then 6 doubles per item
-///   (Gaussian: comp, A, w, cx, cy, cz; Fourier: comp, A, kx, ky, kz, phase).
+///   (Gaussian: comp, A, w, cx, cy, cz; Fourier: comp, A, kx, ky, kz, phase);
+///   kind TS_INIT_EXPRESSION: table[1] = NC, table[2 + c] = start (in doubles) and
+///   table[2 + NC + c] = length (instructions) of component c's postfix program
+///   (treesap::expr::Instr, two doubles each), the programs after the header.
 /// Same formulas and summation order as tsb::GaussianSumInit / tsb::FourierSumInit.
 template <int NC> struct TableInit {
     static constexpr int ncomp = NC;
@@ -37,6 +42,10 @@ template <int NC> struct TableInit {
     template <int c>
     AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE amrex::Real operator()(amrex::Real x, amrex::Real y, amrex::Real z) const {
         const int kind = int(table[0]), n = int(table[1]);
+        if (kind == TS_INIT_EXPRESSION) {
+            const auto* code = reinterpret_cast<const treesap::expr::Instr*>(table + int(table[2 + c]));
+            return treesap::expr::eval(code, int(table[2 + NC + c]), x, y, z);
+        }
         amrex::Real v = 0.0;
         for (int p = 0; p < n; ++p) {
             const double* it = table + 2 + 6 * p;
@@ -57,6 +66,8 @@ struct IntegratorIface {
     virtual ~IntegratorIface() = default;
     virtual int ncomp() const = 0;
     virtual void initialise(int kind, int nitems, const double* items) = 0;
+    /// Expression initial condition: one expression of x, y, z per component.
+    virtual void initialise_expressions(int count, const char* const* exprs) = 0;
     virtual void set_state(const double* src, bool dev) = 0;
     virtual void get_state(double* dst, bool dev) = 0;
     virtual void step() = 0;
@@ -93,6 +104,27 @@ template <class Integ, int NC> class Adapter final : public IntegratorIface {
         host[0] = kind;
         host[1] = nitems;
         for (int q = 0; q < 6 * nitems; ++q) host[2 + q] = items[q];
+        cuda_check(cudaMemcpyAsync(table_, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                   integ_.stream()),
+                   "cudaMemcpyAsync(init table)");
+        integ_.initialise();
+        cuda_check(cudaStreamSynchronize(integ_.stream()), "cudaStreamSynchronize(initialise)");
+    }
+    void initialise_expressions(int count, const char* const* exprs) override {
+        if (count != NC) throw std::invalid_argument("one expression per component is required");
+        std::vector<double> host(2 + 2 * NC);
+        host[0] = TS_INIT_EXPRESSION;
+        host[1] = NC;
+        for (int c = 0; c < NC; ++c) {
+            if (!exprs[c]) throw std::invalid_argument("null expression");
+            const std::vector<treesap::expr::Instr> code = treesap::expr::Compiler::compile(exprs[c]);
+            host[2 + c] = double(host.size());
+            host[2 + NC + c] = double(code.size());
+            const std::size_t at = host.size();
+            host.resize(at + 2 * code.size());
+            std::memcpy(host.data() + at, code.data(), sizeof(treesap::expr::Instr) * code.size());
+        }
+        if (host.size() > table_cap_) throw std::invalid_argument("expressions too long for the parameter table");
         cuda_check(cudaMemcpyAsync(table_, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice,
                                    integ_.stream()),
                    "cudaMemcpyAsync(init table)");

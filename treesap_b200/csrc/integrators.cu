@@ -137,6 +137,24 @@ ts_status ts_integrator_initialise(ts_integrator* it, int init_kind, int nitems,
     return guarded(it->ctx, "ts_integrator_initialise", [&] { it->impl->initialise(init_kind, nitems, items); });
 }
 
+ts_status ts_integrator_initialise_expressions(ts_integrator* it, int count, const char* const* exprs) {
+    if (!it || !it->impl || !exprs || count < 1) return TS_ERR_INVALID_ARGUMENT;
+    return guarded(it->ctx, "ts_integrator_initialise_expressions",
+                   [&] { it->impl->initialise_expressions(count, exprs); });
+}
+
+ts_status ts_expression_eval(const char* expr, int n, const double* x, const double* y, const double* z,
+                             double* out) {
+    if (!expr || n < 0 || (n > 0 && (!x || !y || !z || !out))) return TS_ERR_INVALID_ARGUMENT;
+    try {
+        const std::vector<treesap::expr::Instr> code = treesap::expr::Compiler::compile(expr);
+        for (int q = 0; q < n; ++q) out[q] = treesap::expr::eval(code.data(), int(code.size()), x[q], y[q], z[q]);
+    } catch (const std::exception&) {
+        return TS_ERR_INVALID_ARGUMENT;
+    }
+    return TS_OK;
+}
+
 ts_status ts_integrator_set_state(ts_integrator* it, const double* src, int src_is_device) {
     if (!it || !it->impl || !src) return TS_ERR_INVALID_ARGUMENT;
     return guarded(it->ctx, "ts_integrator_set_state", [&] { it->impl->set_state(src, src_is_device != 0); });
