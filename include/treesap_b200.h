@@ -101,7 +101,9 @@ TS_API ts_status ts_field_tensor_map(const ts_field_layout* layout, const void* 
  *   TS_MODEL_TENSOR_WAVE  {h_ij, p_ij} (2 x SymRank2Alias): h_t = p,
  *                         p_t = Lap h - 1/3 delta Lap tr h + 1/2 (d_i d_k h_kj + d_j d_k h_ki)
  * optionally wrapped in KODecorator{rhs, ko_strength} (order = ngrow) and, when
- * abl_thickness > 0, built as ABLPDEModel (absorbing layer, Dirichlet(target) ghosts). */
+ * abl_thickness > 0, built as ABLPDEModel (absorbing layer, Dirichlet(target) ghosts).
+ * TS_MODEL_TENSOR_WAVE is built for ngrow 3, ko_strength > 0, TS_BC_NOOP, TS_RK4 (FP64 or
+ * FP32-stage), no absorbing layer; other tensor descriptors return TS_ERR_UNSUPPORTED. */
 typedef struct ts_wave_desc {
     int n[3];
     double prob_lo[3];

@@ -32,7 +32,8 @@ def wave_desc_from_golden(d) -> WaveDesc:
     return w
 
 
-@pytest.mark.parametrize("name", [n for n in names() if not n.startswith("tensor")])
+# the library builds the tensor model for ngrow 3 only (its benchmark configuration)
+@pytest.mark.parametrize("name", [n for n in names() if not n.startswith("tensor") or n.endswith("_g3")])
 def test_gpu_reproduces_reference_golden(ctx, name):
     d, inp, nsteps, t, out = load(name)
     w = wave_desc_from_golden(d)

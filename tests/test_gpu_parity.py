@@ -191,3 +191,41 @@ def test_function_init_expressions_match_numpy(ctx):
     np.testing.assert_allclose(got, want, rtol=1e-14, atol=1e-15)
     with pytest.raises(Exception):
         it.initialise_expressions(["exp(", "0"])
+
+
+def tensor_desc(n, precision=TS_F64, dt=None):
+    from treesap_b200 import TS_MODEL_TENSOR_WAVE
+
+    n3 = (n, n, n) if np.isscalar(n) else tuple(n)
+    return wave_desc(n3, 3, periodic=(1, 1, 1), ko=0.1, precision=precision, model=TS_MODEL_TENSOR_WAVE,
+                     dt=dt if dt is not None else 0.25 / n3[0])
+
+
+def test_tensor_model_matches_oracle(ctx, port_oracle):
+    """12-component tensor wave (symmetric-tensor aliases, mixed derivatives, trace) vs the oracle."""
+    d = tensor_desc((20, 17, 23))
+    state = smooth_state(d.shape(), seed=33)
+    it = Integrator(ctx, d)
+    it.set_state(state)
+    it.step(3)
+    gpu = it.get_state()
+    cpu, _, _ = port_oracle.run(d, 3, state=state)
+    assert relerr(gpu, cpu) <= TOL_F64
+
+
+def test_tensor_fp32_stage_error_vs_fp64(ctx):
+    from treesap_b200 import TS_INIT_FOURIER
+
+    rng = np.random.default_rng(3)
+    modes = []
+    for _ in range(12):
+        k = rng.integers(-3, 4, 3)
+        modes.append([rng.integers(0, 6), rng.normal(0, 0.01), *k, rng.uniform(0, 6.28)])
+    out = {}
+    for p in (TS_F64, TS_F32_STAGE):
+        it = Integrator(ctx, tensor_desc(32, p))
+        it.initialise(TS_INIT_FOURIER, np.array(modes, dtype=float))
+        it.step(40)
+        out[p] = it.get_state()
+    ctx.sync()
+    assert relerr(out[TS_F32_STAGE], out[TS_F64]) <= 1e-6

@@ -56,7 +56,9 @@ ts_status validate(const ts_wave_desc* d) {
     if (d->precision == TS_PRECISION_F32_STAGE && d->scheme != TS_RK4) return TS_ERR_UNSUPPORTED;
     if (d->abl_thickness < 0 || (d->abl_thickness > 0 && d->abl_profile != 1 && d->abl_profile != 2))
         return TS_ERR_INVALID_ARGUMENT;
-    if (d->model == TS_MODEL_TENSOR_WAVE && (d->ngrow < 2 || d->ngrow > 3 || d->c2 || d->abl_thickness > 0))
+    // the tensor model is built in its benchmark configuration only (models_tensor_*.cu)
+    if (d->model == TS_MODEL_TENSOR_WAVE && (d->ngrow != 3 || d->c2 || d->abl_thickness > 0 || !(d->ko_strength > 0.0) ||
+                                             d->bc != TS_BC_NOOP || d->scheme != TS_RK4))
         return TS_ERR_UNSUPPORTED;
     return TS_OK;
 }
@@ -96,7 +98,8 @@ ts_status ts_integrator_create(ts_context* ctx, const ts_wave_desc* desc, ts_int
         cuda_check(cudaEventCreate(&it->ev0), "cudaEventCreate");
         cuda_check(cudaEventCreate(&it->ev1), "cudaEventCreate");
         if (desc->model == TS_MODEL_TENSOR_WAVE) {
-            throw std::invalid_argument("the tensor model is not instantiated in this build");
+            it->impl = desc->precision == TS_PRECISION_F32_STAGE ? make_tensor_f32(ctx, *desc, it->table)
+                                                                 : make_tensor_f64(ctx, *desc, it->table);
         } else {
             switch (desc->ngrow) {
             case 1: it->impl = make_wave_g1(ctx, *desc, it->table, it->c2); break;
