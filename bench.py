@@ -18,7 +18,8 @@ steps -> host state out) with the host<->device copies inside the timed region.
 The line also carries `batched`: the C4 workload (512 periodic instances, edges 16..96) through
 ts_batch_* (autotuned launch shape, one persistent launch per stage, CUDA graph), 200 steps, and
 `adjoint`: the C5 loss + gradient through ts_adjoint_* (seconds, and the largest relative
-difference to central finite differences over 32 random directions of phi0 and of c).
+difference to central finite differences over 32 random directions of phi0 and of c), and
+`tensor`: C3 (192^3, 12 components) for a few steps of each form.
 For N > 1 every rank runs an independent replica (weak scaling; the z-slab halo exchange of
 a sharded domain is not part of this build).
 """
@@ -44,6 +45,7 @@ UNIT = "cell-updates/s"
 N = 256
 E2E_CHUNK = 20  # steps per end-to-end call (the plot-export cadence of the reference's driver)
 BATCH_STEPS = 200  # C4 step count
+TENSOR_STEPS = 3  # C3 steps per form (about 1 s per step)
 # Algorithmic HBM bytes per cell and launch (2 components, valid cells only, ghost fills excluded).
 ALG_BYTES = {
     # FP32-stage per component: R u8 W k0 8 W u_p 8 | R k0 8 W d1 4 | R d1 4 W d2 4 | R d2 4, d1 4, u_p 8 W u 8
@@ -342,6 +344,18 @@ def run_b200(args, rank, world, local_rank):
     except Exception as ex:  # noqa: BLE001 - reported in the line
         batched = {"value": None, "error": str(ex)}
 
+    # tensor model (C3): a few steps of each form (the 12-component kernels are slow)
+    tensor = None
+    try:
+        from treesap_b200.run_tensor import run as run_tensor
+
+        r = run_tensor(ctx, steps=TENSOR_STEPS, warmup=1)
+        tensor = {"workload": "C3: 192^3 periodic tensorial wave (h_ij, p_ij; 12 components), ngrow 3, KO 0.1, "
+                              "RK4 dt=0.25dx, 32 seeded Fourier modes", "steps": TENSOR_STEPS,
+                  "fp32_stage": r["f32"], "fp64": r["f64"], "error_f32_vs_f64": r["error_f32_vs_f64"]}
+    except Exception as ex:  # noqa: BLE001 - reported in the line
+        tensor = {"error": str(ex)}
+
     # discrete adjoint (C5): loss + gradient time and central-difference agreement
     adjoint = None
     try:
@@ -383,6 +397,7 @@ def run_b200(args, rank, world, local_rank):
             "clocks_fp64_run": {k: f64["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
             "batched": batched,
             "adjoint": adjoint,
+            "tensor": tensor,
         }
         print(json.dumps(line))
     ctx.close()

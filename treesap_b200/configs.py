@@ -149,3 +149,25 @@ def c5_pulse(n: int = 128, shift_cells: float = 0.0, amplitude: float = 1.0, wid
     z3, y3, x3 = np.meshgrid(x, x, x, indexing="ij")
     cx = 0.5 + shift_cells / n
     return amplitude * np.exp(-((x3 - cx) ** 2 + (y3 - 0.5) ** 2 + (z3 - 0.5) ** 2) / width**2)
+
+
+C3_STEPS = 500
+
+
+def c3_desc(precision: int = TS_F32_STAGE_DEFAULT, n: int = 192) -> WaveDesc:
+    """C3: tensorial wave system (h_ij, p_ij), n^3 periodic unit cube, ngrow 3, KO 0.1, RK4 dt = 0.25 dx."""
+    from . import TS_MODEL_TENSOR_WAVE
+
+    return wave_desc(n, 3, periodic=(1, 1, 1), ko=0.1, precision=precision, model=TS_MODEL_TENSOR_WAVE)
+
+
+def c3_modes(seed: int = 3003, count: int = 32, kmax: int = 8) -> np.ndarray:
+    """h_ij(0) = sum of `count` seeded Fourier modes (component, A ~ N(0, 0.01), integer k, |k| <= kmax, phase)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < count:
+        k = rng.integers(-kmax, kmax + 1, 3)
+        if not k.any() or np.linalg.norm(k) > kmax:
+            continue
+        out.append([rng.integers(0, 6), rng.normal(0.0, 0.01), *k, rng.uniform(0, 2 * np.pi)])
+    return np.array(out, dtype=np.float64)
