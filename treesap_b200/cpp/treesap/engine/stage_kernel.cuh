@@ -41,6 +41,7 @@
 
 #include <cmath>
 #include <cuda_runtime.h>
+#include <utility>
 
 #include "../util/static_for.hpp"
 #include "field.hpp"
@@ -191,6 +192,17 @@ __device__ __forceinline__ void stcs(V* p, const V (&v)[CX], const bool (&act)[C
 #pragma unroll
     for (int e = 0; e < CX; ++e)
         if (act[e]) __stcs(p + e, v[e]);
+}
+
+/// The RHS functor for every component of one cell, in component order, on one workspace
+/// (SingleLevelRK4Integrator.hpp:139-155). A fold rather than a lambda: a lambda that the
+/// compiler declines to inline (many components) would force the register queue that the
+/// Array4's view points at into local memory.
+template <class RHS, class T, int NC, int... C>
+__device__ __forceinline__ void eval_components(const RHS& f, T (&kv)[NC], const amrex::IntVect& idx, double time,
+                                                const amrex::Array4<const T>& arr, const amrex::GeometryData& geom,
+                                                typename RHS::Workspace& ws, std::integer_sequence<int, C...>) {
+    ((kv[C] = static_cast<T>(f.template operator()<C>(idx, time, arr, geom, ws))), ...);
 }
 
 /// One unit of work of a CTA: the tile at (x0, y0) of instance `inst`, planes z0 .. z1-1.
@@ -482,9 +494,7 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
                         arr.view = &view;
                         typename RHS::Workspace ws{};
                         const amrex::IntVect idx{i0 + e, j, z};
-                        treesap::static_for<NC>([&]<int c>() {
-                            kv[u][e][c] = static_cast<T>(f.template operator()<c>(idx, time, arr, geom, ws));
-                        });
+                        eval_components(f, kv[u][e], idx, time, arr, geom, ws, std::make_integer_sequence<int, NC>{});
                     }
                 }
             }

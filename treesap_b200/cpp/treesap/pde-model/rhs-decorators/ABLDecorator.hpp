@@ -5,6 +5,7 @@
 #pragma once
 
 #include <cmath>
+#include <type_traits>
 
 #include "../../util/stencil.hpp"
 #include "../PDEModelConcepts.hpp"
@@ -58,7 +59,7 @@ struct ABLDecorator {
                                                           const amrex::Array4<const T>& arr,
                                                           const amrex::GeometryData& geom, Workspace& ws) const {
         if (!ws.have_sigma) {
-            ws.sigma_value = sigma(idx);
+            ws.sigma_value = sigma_in<T>(idx);
             ws.have_sigma = true;
         }
         return T(rhs.template operator()<comp>(idx, time, arr, geom, ws.inner)) -
@@ -77,6 +78,23 @@ struct ABLDecorator {
         const amrex::Real dist = std::sqrt(static_cast<amrex::Real>(d2));
         const amrex::Real s = amrex::Clamp(data.inv_thickness * dist, 0.0, 1.0);
         return data.max_strength * data.profile(s);
+    }
+
+    /// sigma for stage arithmetic in T: the distance in single precision for T = float (the
+    /// FP32-stage form's stages carry single-precision data anyway), else sigma().
+    template <typename T> AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE amrex::Real sigma_in(const amrex::IntVect& idx) const {
+        if constexpr (std::is_same_v<T, float>) {
+            int d2 = 0;
+            for (int d = 0; d < 3; ++d) {
+                const int v = idx[d] - amrex::Clamp(idx[d], bulk.smallEnd(d), bulk.bigEnd(d));
+                d2 += v * v;
+            }
+            if (d2 == 0) return 0.0;
+            const float s = fminf(float(data.inv_thickness) * sqrtf(float(d2)), 1.0f);
+            return data.max_strength * data.profile(amrex::Real(s));
+        } else {
+            return sigma(idx);
+        }
     }
 
     /// Linear part: the same damping towards zero (targets removed) around the inner linear part.
