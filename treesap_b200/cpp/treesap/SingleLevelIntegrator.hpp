@@ -80,11 +80,12 @@ template <typename T, int G, int NC> struct DefaultTile {
     using Spec = std::conditional_t<sizeof(T) == 8, TileSpec<TREESAP_B200_TILE_F64>, TileSpec<TREESAP_B200_TILE_F32>>;
     template <int CX, int TY, int P, int MINB, int U> using C = treesap_b200::TileCfg<CX, TY, G, NC, T, P, MINB, U>;
     using Pref = C<Spec::CX, Spec::TY, Spec::P, Spec::MINB, Spec::U>;
-    using type =
-        std::conditional_t<Pref::fits, Pref,
-                           std::conditional_t<C<1, 3, 2, 2, 1>::fits, C<1, 3, 2, 2, 1>,
-                                              std::conditional_t<C<1, 3, 2, 1, 1>::fits, C<1, 3, 2, 1, 1>,
-                                                                 C<1, 1, 1, 1, 1>>>>;
+    using type = std::conditional_t<
+        Pref::fits, Pref,
+        std::conditional_t<
+            C<1, 3, 2, 2, 1>::fits, C<1, 3, 2, 2, 1>,
+            std::conditional_t<C<1, 3, 2, 1, 1>::fits, C<1, 3, 2, 1, 1>,
+                               std::conditional_t<C<1, 2, 1, 1, 1>::fits, C<1, 2, 1, 1, 1>, C<1, 1, 1, 1, 1>>>>>;
 };
 } // namespace detail
 
