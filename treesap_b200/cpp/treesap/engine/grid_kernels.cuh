@@ -104,7 +104,7 @@ __global__ void ghost_fill_kernel(T* __restrict__ f, const Layout L, const amrex
         ghost_fill_cell(f, L, geom, bc, bcr, time, mode, t);
 }
 
-/// One field of a batched ghost fill; `first` = ghost cells of all earlier entries.
+/// One field of a batched ghost fill.
 template <class T, class BC> struct GhostEntry {
     T* f;
     Layout L;
@@ -112,24 +112,33 @@ template <class T, class BC> struct GhostEntry {
     BC bc;
     double time;
     int mode;
-    long long first;
 };
 
-/// Ghost fill of many fields in one launch: thread t of the grid-stride loop fills ghost cell
-/// t - first of the entry whose range holds t (binary search over the entries' `first`).
+/// A run of `kGhostChunk` consecutive ghost cells (or fewer, at the end) of one entry.
+struct GhostChunk {
+    int entry;
+    int pad;
+    long long first;
+};
+constexpr int kGhostChunk = 2048;
+
+/// Ghost fill of many fields in one launch: block b fills the ghost cells of chunk b (its
+/// entry read once per block from global memory into shared memory).
 template <class T, class BC>
-__global__ void batch_ghost_fill_kernel(const GhostEntry<T, BC>* __restrict__ entries, int count, long long total,
-                                        const amrex::BCRec* bcr) {
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
-        int lo = 0, hi = count - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) / 2;
-            if (entries[mid].first <= t) lo = mid;
-            else hi = mid - 1;
-        }
-        const GhostEntry<T, BC>& e = entries[lo];
-        ghost_fill_cell(e.f, e.L, e.geom, e.bc, bcr, e.time, e.mode, t - e.first);
+__global__ void __launch_bounds__(256) batch_ghost_fill_kernel(const GhostEntry<T, BC>* __restrict__ entries,
+                                                              const GhostChunk* __restrict__ chunks, int nchunks,
+                                                              const amrex::BCRec* bcr) {
+    __shared__ __align__(16) unsigned char raw[sizeof(GhostEntry<T, BC>)];
+    auto& e = *reinterpret_cast<GhostEntry<T, BC>*>(raw);
+    for (int b = blockIdx.x; b < nchunks; b += gridDim.x) {
+        const GhostChunk ch = chunks[b];
+        __syncthreads(); // the previous chunk's threads are done with the entry
+        if (threadIdx.x == 0) e = entries[ch.entry];
+        __syncthreads();
+        const long long total = ghost_count(e.L).total();
+        const long long end = ch.first + kGhostChunk < total ? ch.first + kGhostChunk : total;
+        for (long long t = ch.first + threadIdx.x; t < end; t += blockDim.x)
+            ghost_fill_cell(e.f, e.L, e.geom, e.bc, bcr, e.time, e.mode, t);
     }
 }
 

@@ -334,13 +334,12 @@ class BatchedRK4Integrator {
 
     template <class T> struct FillPlan {
         DevArray<treesap_b200::GhostEntry<T, BCType>> entries;
-        long long total = 0;
+        DevArray<treesap_b200::GhostChunk> chunks;
         void launch(const amrex::BCRec* bcr, int sms, cudaStream_t s) const {
-            if (total == 0) return;
-            long long blocks = (total + 255) / 256;
-            if (blocks > 16LL * sms) blocks = 16LL * sms;
-            treesap_b200::batch_ghost_fill_kernel<T, BCType>
-                <<<int(blocks), 256, 0, s>>>(entries.p, entries.n, total, bcr);
+            if (chunks.n == 0) return;
+            int blocks = chunks.n;
+            if (blocks > 32 * sms) blocks = 32 * sms;
+            treesap_b200::batch_ghost_fill_kernel<T, BCType><<<blocks, 256, 0, s>>>(entries.p, chunks.p, chunks.n, bcr);
             treesap_b200::cuda_check(cudaGetLastError(), "batch_ghost_fill_kernel launch");
         }
     };
@@ -447,15 +446,15 @@ class BatchedRK4Integrator {
     template <class T> void build_fill(FillPlan<T>& f, std::vector<std::pair<T*, treesap_b200::Layout>> fields,
                                        treesap_b200::GhostMode mode) {
         std::vector<treesap_b200::GhostEntry<T, BCType>> h;
-        long long first = 0;
+        std::vector<treesap_b200::GhostChunk> ch;
         for (int i = 0; i < size(); ++i) {
-            treesap_b200::GhostEntry<T, BCType> e{fields[i].first, fields[i].second, insts[i].geom,
-                                                  models[i].get_bc(), insts[i].time, int(mode), first};
-            first += treesap_b200::ghost_count(fields[i].second).total();
-            h.push_back(e);
+            h.push_back(treesap_b200::GhostEntry<T, BCType>{fields[i].first, fields[i].second, insts[i].geom,
+                                                            models[i].get_bc(), insts[i].time, int(mode)});
+            const long long total = treesap_b200::ghost_count(fields[i].second).total();
+            for (long long c = 0; c < total; c += treesap_b200::kGhostChunk) ch.push_back({i, 0, c});
         }
         f.entries.upload(h, stream());
-        f.total = first;
+        f.chunks.upload(ch, stream());
     }
 
     void ensure_plans() {
@@ -594,12 +593,19 @@ class BatchedRK4Integrator {
             P.s2.entries.release();
             P.s3.entries.release();
             if constexpr (F32Stage) {
-                P.fill_u.entries.release();
-                P.fill_k0.entries.release();
-                P.fill_d1.entries.release();
-                P.fill_d2.entries.release();
+                for (auto* f : {&P.fill_u, &P.fill_k0}) {
+                    f->entries.release();
+                    f->chunks.release();
+                }
+                for (auto* f : {&P.fill_d1, &P.fill_d2}) {
+                    f->entries.release();
+                    f->chunks.release();
+                }
             } else {
-                for (auto& f : P.fill) f.entries.release();
+                for (auto& f : P.fill) {
+                    f.entries.release();
+                    f.chunks.release();
+                }
             }
         }
     }
