@@ -367,7 +367,10 @@ def run_b200(args, rank, world, local_rank):
                    "gradient_seconds": a["gradient_s"], "forward_seconds": a["forward_s"],
                    "gradient_over_forward": a["gradient_s"] / a["forward_s"],
                    "fd_directions": a["directions"], "fd_rel_err_max_phi0": a["fd_rel_max_phi0"],
-                   "fd_rel_err_max_c": a["fd_rel_max_c"], "tolerance": 1e-5}
+                   "fd_rel_err_max_c": a["fd_rel_max_c"], "tolerance": 1e-5,
+                   "fp32_stage": {"state_gradient_seconds": a["fp32_stage_state_gradient_s"],
+                                  "grad_phi0_maxnorm_rel_vs_fp64": a["fp32_stage_grad_phi0_rel_vs_fp64"],
+                                  "loss_rel_vs_fp64": a["fp32_stage_loss_rel_vs_fp64"]}}
     except Exception as ex:  # noqa: BLE001 - reported in the line
         adjoint = {"error": str(ex)}
 

@@ -100,3 +100,37 @@ def test_adjoint_rejects_unsupported(ctx):
     with pytest.raises(TSError) as e:
         Adjoint(ctx, wave_desc(16, 3, periodic=(1, 1, 1)))
     assert e.value.status == 2
+
+
+def relmax(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+@pytest.mark.parametrize("ngrow", [2, 4])
+def test_fp32_stage_state_gradient_vs_fp64(ctx, ngrow):
+    """FP32-stage forward run and reverse sweep: loss and initial-state gradients within 1e-6 of FP64."""
+    d, c, phi0, pi0, target = setup(24, ngrow)
+    adj = Adjoint(ctx, d, 5)
+    l64, g64, p64, _ = adj.gradient(phi0, pi0, c, 20, target)
+    l32, g32, p32 = adj.gradient_f32(phi0, pi0, c, 20, target)
+    assert abs(l32 - l64) <= 1e-6 * abs(l64)
+    assert relmax(g32, g64) <= 1e-6 and relmax(p32, p64) <= 1e-6
+
+
+def test_fp32_stage_state_gradient_matches_central_differences(ctx):
+    d, c, phi0, pi0, target = setup(20, 2)
+    adj = Adjoint(ctx, d, 5)
+    _, g32, _ = adj.gradient_f32(phi0, pi0, c, 12, target)
+    rng = np.random.default_rng(5)
+    for _ in range(3):
+        v = rng.standard_normal(phi0.shape)
+        v /= np.linalg.norm(v)
+        # J is quadratic in the initial state, so the central difference carries no truncation
+        # error at any step; a wide step keeps the FP32-stage rounding of J (about 1e-8 of J)
+        # small against the difference itself.
+        eps = 0.1
+        lp = adj.gradient_f32(phi0 + eps * v, pi0, c, 12, target)[0]
+        lm = adj.gradient_f32(phi0 - eps * v, pi0, c, 12, target)[0]
+        fd = (lp - lm) / (2 * eps)
+        ad = float(np.sum(g32 * v))
+        assert abs(fd - ad) <= 1e-5 * abs(ad), (fd, ad)

@@ -163,6 +163,7 @@ def lib() -> C.CDLL:
         "ts_adjoint_forward": (i, [vp, vp, vp, vp, i, vp, vp]),
         "ts_adjoint_gradient": (i, [vp, vp, vp, vp, i, vp, C.POINTER(d), vp, vp, vp]),
         "ts_adjoint_tangent": (i, [vp, vp, vp, vp, vp, vp, vp, i, vp, vp]),
+        "ts_adjoint_gradient_f32": (i, [vp, vp, vp, vp, i, vp, C.POINTER(d), vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -414,6 +415,16 @@ class Adjoint:
                                          C.byref(loss), _ptr(gphi), _ptr(gpi), _ptr(gc)),
                "ts_adjoint_gradient", self.ctx)
         return loss.value, gphi, gpi, gc
+
+    def gradient_f32(self, phi0, pi0, c, nsteps: int, target):
+        """FP32-stage form: (J, dJ/dphi0, dJ/dpi0)."""
+        phi0, pi0, c, target = self._in(phi0), self._in(pi0), self._in(c), self._in(target)
+        gphi, gpi = np.empty(self.shape), np.empty(self.shape)
+        loss = C.c_double()
+        _check(lib().ts_adjoint_gradient_f32(self.handle, _ptr(phi0), _ptr(pi0), _ptr(c), nsteps, _ptr(target),
+                                             C.byref(loss), _ptr(gphi), _ptr(gpi)),
+               "ts_adjoint_gradient_f32", self.ctx)
+        return loss.value, gphi, gpi
 
     def tangent(self, phi0, pi0, c, dphi0, dpi0, dc, nsteps: int):
         args = [self._in(a) for a in (phi0, pi0, c, dphi0, dpi0, dc)]

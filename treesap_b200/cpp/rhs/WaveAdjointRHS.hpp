@@ -136,6 +136,54 @@ template <int ngrow_> struct WaveC2LaplacianRHS {
     }
 };
 
+/// Adjoint model {phibar, pibar} with the speed as a coefficient field instead of a state
+/// component: phibar_t = s K phibar + D (c2 pibar), pibar_t = phibar + s K pibar, c2 read from a
+/// device array of the valid cells (x fastest) with periodic wrap-around at the neighbour taps.
+/// Linear in the state, so it also runs in the FP32-stage RK4 form (whose stage differences
+/// would lose a coefficient carried as a state component).
+template <int ngrow_> struct WaveAdjointSpeedRHS {
+    static constexpr int ncomp = 2;
+    static constexpr int ngrow = ngrow_;
+    static constexpr bool is_affine_autonomous = true;
+    struct Workspace {};
+    const double* c2 = nullptr;
+    int n[3] = {0, 0, 0};
+    amrex::Real ko_strength = 0.0;
+
+    template <int comp, typename T>
+    AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE T operator()(const amrex::IntVect idx, amrex::Real,
+                                                          const amrex::Array4<const T>& arr,
+                                                          const amrex::GeometryData& geom, Workspace&) const {
+        const T ko = ko_strength > 0.0 ? detail::ko_sum<ngrow>(arr, comp, idx, geom) : T(0);
+        T base;
+        if constexpr (comp == 0) {
+            using namespace treesap::stencil_impl;
+            const int i = idx[0], j = idx[1], k = idx[2];
+            auto wrap = [](int a, int m) { return a < 0 ? a + m : (a >= m ? a - m : a); };
+            auto f = [&](int a, int b, int c) {
+                const long long q = wrap(a, n[0]) + (long long)n[0] * (wrap(b, n[1]) + (long long)n[1] * wrap(c, n[2]));
+                return T(c2[q]) * arr(a, b, c, 1);
+            };
+            base = T(0);
+            treesap::static_for<3>([&]<int d>() {
+                using U = treesap::stencil_impl::detail::Unit<d>;
+                const amrex::Real gf = 1.0 / (geom.CellSize(d) * geom.CellSize(d));
+                constexpr T w0 = T(weights::second<ngrow>(0));
+                T acc = w0 * f(i, j, k);
+                treesap::static_for<1, ngrow + 1>([&]<int s>() {
+                    constexpr T w = T(weights::second<ngrow>(s));
+                    acc += w * (f(i + s * U::x, j + s * U::y, k + s * U::z) +
+                                f(i - s * U::x, j - s * U::y, k - s * U::z));
+                });
+                base += T(gf) * acc;
+            });
+        } else {
+            base = arr(idx, 0);
+        }
+        return ko_strength > 0.0 ? base + T(ko_strength) * ko : base;
+    }
+};
+
 /// Tangent-linear model {phi, pi, c2, dphi, dpi, dc2}.
 template <int ngrow_> struct WaveC2TangentRHS {
     static constexpr int ncomp = 6;

@@ -41,6 +41,8 @@
 
 #include <cmath>
 #include <cuda_runtime.h>
+#include <stdexcept>
+#include <string>
 #include <utility>
 
 #include "../util/static_for.hpp"
@@ -847,7 +849,10 @@ template <class Cfg, class RHS, class Epi> struct StageLauncher {
         sp.zchunk = s.zchunk;
         const int threads = 32 * s.ty + 32;
         stage_kernel<Cfg, RHS, Epi><<<s.grid, threads, RingT::SMEM, stream>>>(tmap, cmaps, sp, rhs, ep);
-        cuda_check(cudaGetLastError(), "stage_kernel launch");
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess)
+            throw std::runtime_error(std::string("stage_kernel launch (") + __PRETTY_FUNCTION__ +
+                                     "): " + cudaGetErrorString(e));
     }
 };
 

@@ -227,6 +227,8 @@ IntegratorIface* make_wave_g1(ts_context*, const ts_wave_desc&, double* table, c
 IntegratorIface* make_wave_g2(ts_context*, const ts_wave_desc&, double* table, const double* c2);
 IntegratorIface* make_wave_g3(ts_context*, const ts_wave_desc&, double* table, const double* c2);
 IntegratorIface* make_wave_g4(ts_context*, const ts_wave_desc&, double* table, const double* c2);
+IntegratorIface* make_wave_adjoint_g2(ts_context*, const ts_wave_desc&, double* table, const double* c2);
+IntegratorIface* make_wave_adjoint_g4(ts_context*, const ts_wave_desc&, double* table, const double* c2);
 IntegratorIface* make_tensor_f64(ts_context*, const ts_wave_desc&, double* table);
 IntegratorIface* make_tensor_f32(ts_context*, const ts_wave_desc&, double* table);
 

@@ -6,7 +6,8 @@
 4th-order stencils, KO 0.1, RK4 200 steps; loss J = 1/2 sum (phi(T) - phi_target)^2 with
 phi_target from a forward run of the pulse shifted by 2 cells and scaled by 1.05. Prints the
 time of one loss+gradient evaluation and, per random unit direction v of phi0 and of c, the
-relative difference between <grad, v> and (J(p + eps v) - J(p - eps v)) / (2 eps).
+relative difference between <grad, v> and (J(p + eps v) - J(p - eps v)) / (2 eps); then the
+FP32-stage form of the initial-state gradient (time, and its difference to the FP64 one).
 """
 from __future__ import annotations
 
@@ -50,10 +51,18 @@ def run(ctx, n=128, steps=C5_STEPS, every=C5_CHECKPOINT_EVERY, directions=32, se
                 fd = (J(phi0, c + eps * v) - J(phi0, c - eps * v)) / (2 * eps)
             ad = float(np.sum(g * v))
             rel[name].append(abs(fd - ad) / abs(ad))
+    # FP32-stage form of the initial-state gradient
+    adj.gradient_f32(phi0, pi0, c, steps, target)  # warm-up
+    t0 = time.perf_counter()
+    loss32, gphi32, _ = adj.gradient_f32(phi0, pi0, c, steps, target)
+    t_grad32 = time.perf_counter() - t0
+    rel32 = float(np.abs(gphi32 - gphi).max() / np.abs(gphi).max())
     adj.close()
     return {"loss": loss, "cells": n**3, "steps": steps, "checkpoint_every": every, "gradient_s": t_grad,
             "forward_s": t_fwd, "fd_rel_max_phi0": max(rel["phi0"]), "fd_rel_max_c": max(rel["c"]),
-            "directions": directions}
+            "directions": directions, "fp32_stage_state_gradient_s": t_grad32,
+            "fp32_stage_grad_phi0_rel_vs_fp64": rel32,
+            "fp32_stage_loss_rel_vs_fp64": abs(loss32 - loss) / abs(loss)}
 
 
 def main() -> None:
