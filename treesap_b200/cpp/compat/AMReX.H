@@ -150,11 +150,16 @@ template <class U> struct StencilView {
     int ci, cj, ck;
     int pjs, pns;    // shared-memory plane row and component strides
     int qg, qnc;     // register queue half-depth and component count
+    int qrot = 0;    // circular queue (qlen > 0): offset k + dk sits in slot (dk + qg + qrot) % qlen
+    int qlen = 0;
 
     AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE const U& at(int i, int j, int k, int n) const {
         const int di = i - ci, dj = j - cj, dk = k - ck;
         if (dk == 0) return plane[n * pns + dj * pjs + di];
-        if (di == 0 && dj == 0 && dk >= -qg && dk <= qg && n < qnc) return queue[(dk + qg) * qnc + n];
+        if (di == 0 && dj == 0 && dk >= -qg && dk <= qg && n < qnc) {
+            const int m = dk + qg + qrot;
+            return queue[(qlen > 0 ? m % qlen : m) * qnc + n];
+        }
         return glob[n * gns + dk * gks + dj * gjs + di];
     }
 };

@@ -62,8 +62,9 @@ struct KernelClock {
 namespace detail {
 /// Tile shape of the fused stage kernel for a value type, ghost width and component count:
 /// CX cells per thread along x, TY rows (consumer warps) plus the producer warp, P planes of
-/// prefetch, MINB CTAs per SM, U planes per iteration; TREESAP_B200_TILE_F64 / _F32 override
-/// the defaults at build time as the decimal number CX TY(2 digits) P MINB U, e.g. 107222;
+/// prefetch, MINB CTAs per SM, U planes per iteration, CY rows per consumer warp;
+/// TREESAP_B200_TILE_F64 / _F32 override the defaults at build time as the decimal number
+/// [CY] CX TY(2 digits) P MINB U, e.g. 107222 (CY = 1) or 2105421;
 /// when two FP64 centre-operand fields would not fit the shared-memory budget (many
 /// components), narrower tiles.
 #ifndef TREESAP_B200_TILE_F64
@@ -72,14 +73,26 @@ namespace detail {
 #ifndef TREESAP_B200_TILE_F32
 #define TREESAP_B200_TILE_F32 207421
 #endif
+// Circular register queue (TileCfg::ROT) for FP64 / FP32 stencil inputs of at most 4
+// components: it removes the per-plane queue shift (16 moves per FP64 component and cell at
+// ngrow 4) at the price of a plane loop unrolled 2 ngrow + 1 times. Measured at 256^3, ngrow 4:
+// FP64 stages 3-10% faster; FP32 stages (two cells per thread) 30% slower, so off for FP32.
+#ifndef TREESAP_B200_QROT_F64
+#define TREESAP_B200_QROT_F64 1
+#endif
+#ifndef TREESAP_B200_QROT_F32
+#define TREESAP_B200_QROT_F32 0
+#endif
 template <int code> struct TileSpec {
-    static constexpr int CX = code / 100000, TY = code / 1000 % 100, P = code / 100 % 10, MINB = code / 10 % 10,
-                         U = code % 10;
+    static constexpr int CY = code / 1000000 > 0 ? code / 1000000 : 1, CX = code / 100000 % 10,
+                         TY = code / 1000 % 100, P = code / 100 % 10, MINB = code / 10 % 10, U = code % 10;
 };
 template <typename T, int G, int NC> struct DefaultTile {
     using Spec = std::conditional_t<sizeof(T) == 8, TileSpec<TREESAP_B200_TILE_F64>, TileSpec<TREESAP_B200_TILE_F32>>;
-    template <int CX, int TY, int P, int MINB, int U> using C = treesap_b200::TileCfg<CX, TY, G, NC, T, P, MINB, U>;
-    using Pref = C<Spec::CX, Spec::TY, Spec::P, Spec::MINB, Spec::U>;
+    static constexpr bool kRot = (sizeof(T) == 8 ? TREESAP_B200_QROT_F64 : TREESAP_B200_QROT_F32) != 0 && NC <= 4;
+    template <int CX, int TY, int P, int MINB, int U, int CY = 1>
+    using C = treesap_b200::TileCfg<CX, TY, G, NC, T, P, MINB, U, CY, kRot && U == 1>;
+    using Pref = C<Spec::CX, Spec::TY, Spec::P, Spec::MINB, Spec::U, Spec::CY>;
     using type = std::conditional_t<
         Pref::fits, Pref,
         std::conditional_t<

@@ -3,21 +3,22 @@
 // One launch evaluates one stage of the integrator over the whole box. The grid is
 // (x-y tiles) x (z chunks), z-major: CTA b owns tile b % ntiles and z chunk b / ntiles, so the
 // CTAs resident at any time hold neighbouring tiles at the same z and their halo re-reads hit
-// in L2. A CTA has TY consumer warps (one 32-cell x row each, TY <= TYMAX chosen at launch) and
-// one producer warp. Per z plane:
+// in L2. A CTA has TY consumer warps (CY rows of TX = 32 CX cells each, TY <= TYMAX chosen at
+// launch) and one producer warp. Per z plane:
 //
 //   * the producer warp's elected lane copies the plane's tile plus its ghost halo, all
 //     components, with one TMA load (cp.async.bulk.tensor.4d, no multicast; box
-//     (TX+2*XH) x (TY+2G) x 1 x NC, zero fill outside the array) into a ring of R shared-memory
+//     (TX+2*XH) x (TY*CY+2G) x 1 x NC, zero fill outside the array) into a ring of R shared-memory
 //     slots. When the plane is also a stencil centre plane of this CTA, the same slot receives
 //     the epilogue's centre operands (the stage registers it reads at the centre cells, e.g.
-//     the RK4 accumulator and initial state): one more TMA box (TX x TY x 1 x NC) per operand
+//     the RK4 accumulator and initial state): one more TMA box (TX x TY*CY x 1 x NC) per operand
 //     field, completing on the same barrier. Slot s has a `full` mbarrier (TMA transaction
 //     count) and an `empty` mbarrier (one arrival per consumer warp); the producer refills a
 //     slot once every consumer warp has released it, running up to R - G - 1 planes ahead of
 //     the queue and R - 1 planes ahead of the centre computation.
-//   * each consumer thread keeps its column's values at z-G .. z+G in a register queue,
-//     shifted once per plane and fed from the newest plane.
+//   * each consumer thread keeps its CX x CY columns' values at z-G .. z+G in a register
+//     queue, shifted once per plane and fed from the newest plane. The CY rows of a thread
+//     share their y taps (rows j0-G .. j0+CY-1+G), which the compiler loads once.
 //   * the user's RHS functor is called once per component, in component order, on an Array4
 //     whose StencilView resolves every access at compile time: same-z offsets to the
 //     shared-memory plane, same-column offsets to the register queue, anything else
@@ -54,21 +55,26 @@ namespace treesap_b200 {
 constexpr int align128(int b) { return (b + 127) / 128 * 128; }
 
 /// Tile configuration of the stage kernel: CX cells per thread along x (a warp covers
-/// TX = 32 CX cells of a row), up to TYMAX rows (consumer warps), ghost width G, NC components
-/// of type T, up to P planes of prefetch, MINB resident CTAs per SM, U planes per iteration of
-/// the plane loop.
-template <int CX_, int TYMAX_, int G_, int NC_, typename T_, int P_ = 2, int MINB_ = 2, int U_ = 1> struct TileCfg {
+/// TX = 32 CX cells of a row), CY rows per consumer warp, up to TYMAX consumer warps (a tile
+/// is ty * CY rows high), ghost width G, NC components of type T, up to P planes of prefetch,
+/// MINB resident CTAs per SM, U planes per iteration of the plane loop.
+template <int CX_, int TYMAX_, int G_, int NC_, typename T_, int P_ = 2, int MINB_ = 2, int U_ = 1, int CY_ = 1,
+          bool ROT_ = false>
+struct TileCfg {
     using T = T_;
-    static constexpr int CX = CX_, TX = 32 * CX_, TYMAX = TYMAX_, G = G_, NC = NC_, P = P_, U = U_;
+    static constexpr int CX = CX_, TX = 32 * CX_, TYMAX = TYMAX_, G = G_, NC = NC_, P = P_, U = U_, CY = CY_;
+    /// Circular register queue: the plane loop is unrolled by the queue depth 2G + 1 so that
+    /// every plane keeps its register slot (plane % (2G + 1)) instead of being shifted.
+    static constexpr bool ROT = ROT_;
     static constexpr int MIN_BLOCKS = MINB_; // resident CTAs per SM the register and smem budgets are sized for
     static constexpr int A = 16 / int(sizeof(T));   // elements per 16 bytes
     static constexpr int XH = (G + A - 1) / A * A;  // x halo width in shared memory (16-byte aligned)
     static constexpr int BX = TX + 2 * XH;
-    static constexpr int BYMAX = TYMAX + 2 * G;
+    static constexpr int BYMAX = TYMAX * CY + 2 * G;
     static constexpr int PLANE_MAX = NC * BYMAX * BX;  // stencil elements per slot (at TYMAX)
     static constexpr int THREADS = 32 * TYMAX + 32;    // consumer warps + one producer warp
     static constexpr int STENCIL_BYTES = align128(PLANE_MAX * int(sizeof(T)));
-    static constexpr int CBOX = NC * TYMAX * TX;       // elements of one centre-operand box
+    static constexpr int CBOX = NC * TYMAX * CY * TX;  // elements of one centre-operand box
     /// Dynamic shared memory per CTA when MIN_BLOCKS CTAs share an SM (228 KB per SM with 1 KB
     /// reserved per CTA; at most 227 KB for one CTA).
     static constexpr int SMEM_BUDGET = MINB_ == 1 ? 232448 : 233472 / MINB_ - 1024;
@@ -81,15 +87,17 @@ template <int CX_, int TYMAX_, int G_, int NC_, typename T_, int P_ = 2, int MIN
     static constexpr bool fits = smem_for(1, 2 * align128(CBOX * 8)) <= SMEM_BUDGET;
     static_assert(CX == 1 || CX == 2, "one or two cells per thread along x");
     static_assert(U == 1 || U == 2, "one or two planes per iteration");
+    static_assert(CY >= 1 && CY <= 4, "one to four rows per consumer warp");
+    static_assert(!ROT || U == 1, "the circular queue takes one plane per iteration");
     static_assert(BX <= 256 && BYMAX <= 256 && NC <= 256, "TMA box dimensions are limited to 256");
     static_assert(THREADS <= 1024, "too many threads");
 };
 
 /// Shared-memory rings of one (tile configuration, epilogue) pair:
-///   * the stencil ring, R = G + U + P slots, each one stencil plane ([comp][y][x], TY + 2G
+///   * the stencil ring, R = G + U + P slots, each one stencil plane ([comp][y][x], TY CY + 2G
 ///     rows of BX), with a `full` and an `empty` mbarrier per slot;
 ///   * the centre-operand ring, RC = U + P slots (none without centre operands), each the
-///     epilogue's centre-operand boxes of one centre plane ([comp][y][x], TY rows of TX per
+///     epilogue's centre-operand boxes of one centre plane ([comp][y][x], TY CY rows of TX per
 ///     field, 128-byte aligned), with an `empty` mbarrier per slot. The boxes of centre plane
 ///     c are copied together with (and complete on the `full` barrier of) stencil plane c + G,
 ///     the newest plane of the iteration that computes centre plane c.
@@ -124,12 +132,12 @@ template <typename T> struct StageParams {
     amrex::GeometryData geom; // passed to the RHS
     double time;              // stage time t + c_s dt
     int ntx, nty;             // tiles in x and y
-    int ty;                   // tile height (rows = consumer warps), <= TYMAX
+    int ty;                   // consumer warps (a tile is ty * CY rows high), <= TYMAX
     int zchunk;               // planes per z chunk
     int* err;                 // device error word
 };
 
-/// TMA descriptors of the centre-operand fields (box TX x ty x 1 x NC) and the storage
+/// TMA descriptors of the centre-operand fields (box TX x ty CY x 1 x NC) and the storage
 /// coordinates of cell (0, 0, 0) in each (x = xoff, y = z = ngrow).
 struct alignas(64) CentreMaps {
     CUtensorMap map[2];
@@ -227,7 +235,8 @@ template <class Cfg, class RHS, class Epi> struct SingleSource {
         const int ntiles = sp->ntx * sp->nty;
         const int tile = blockIdx.x % ntiles;
         const int z0 = (blockIdx.x / ntiles) * sp->zchunk;
-        return {0, (tile % sp->ntx) * Cfg::TX, (tile / sp->ntx) * sp->ty, z0, min(sp->L.n[2], z0 + sp->zchunk)};
+        return {0, (tile % sp->ntx) * Cfg::TX, (tile / sp->ntx) * sp->ty * Cfg::CY, z0,
+                min(sp->L.n[2], z0 + sp->zchunk)};
     }
     __device__ __forceinline__ int count() const {
         const ItemBox b = first();
@@ -290,10 +299,11 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
     uint64_t* empty = full + R;
     uint64_t* cempty = empty + R;
 
-    const int TY = src.ty();
-    const int BY = TY + 2 * G;
-    const int PNS = BY * BX; // component stride of the stencil plane inside a slot
-    const int CPS = TY * TX; // component stride of a centre-operand box
+    constexpr int CY = Cfg::CY;
+    const int TY = src.ty();      // consumer warps
+    const int BY = TY * CY + 2 * G;
+    const int PNS = BY * BX;      // component stride of the stencil plane inside a slot
+    const int CPS = TY * CY * TX; // component stride of a centre-operand box
     const int nitems = src.count();
     if (nitems == 0) return;
     int* const err = src.err();
@@ -314,8 +324,8 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
         if (lane == 0) {
             const uint32_t bytes = uint32_t(NC * BY * BX * int(sizeof(T)));
             uint32_t cbytes = 0;
-            if constexpr (NCEN > 0) cbytes += uint32_t(NC * TY * TX * int(sizeof(C0)));
-            if constexpr (NCEN > 1) cbytes += uint32_t(NC * TY * TX * int(sizeof(C1)));
+            if constexpr (NCEN > 0) cbytes += uint32_t(CPS * NC * int(sizeof(C0)));
+            if constexpr (NCEN > 1) cbytes += uint32_t(CPS * NC * int(sizeof(C1)));
             // Plane t (counted over all items) goes to stencil slot ps.s once plane t - R is
             // released (completion t / R of empty[ps.s], parity ps.ph ^ 1). From an item's plane
             // q = 2G on, the same transaction carries the centre operands of its centre plane
@@ -379,10 +389,11 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
 
     // -------------------------------------------------------------------- consumer warps
     constexpr int CX = Cfg::CX, U = Cfg::U;
-    constexpr int QL = 2 * G + U; // register queue depth (planes)
+    constexpr int QL = 2 * G + U;  // register queue depth (planes)
+    constexpr int NCOL = CY * CX;  // columns (cells per plane) of a thread: column r CX + e is cell (i0 + e, j0 + r)
     const int tx = lane, ty = warp;
-    const int coff = (ty + G) * BX + (CX * tx + XH); // cell 0's centre inside the stencil plane
-    const int cc = ty * TX + CX * tx;                // ... inside a centre-operand box
+    const int coff = (CY * ty + G) * BX + (CX * tx + XH); // cell (i0, j0)'s centre inside the stencil plane (row r: + r BX)
+    const int cc = CY * ty * TX + CX * tx;                // ... inside a centre-operand box (row r: + r TX)
 
     RingPos pos;  // stencil slot of the item's plane it
     RingPos kpos; // centre slot of the item's centre plane it - G
@@ -401,19 +412,21 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
         const typename Epi::Params epl = src.epi(b.inst);
 
         const int NP = (b.z1 - b.z0) + 2 * G;
-        const int i0 = b.x0 + CX * tx, j = b.y0 + ty; // this thread's cells: (i0 + e, j), e < CX
-        bool act[CX];
+        const int i0 = b.x0 + CX * tx, j0 = b.y0 + CY * ty; // this thread's cells: (i0 + e, j0 + r)
+        bool act[CY][CX];
 #pragma unroll
-        for (int e = 0; e < CX; ++e) act[e] = (i0 + e < L.n[0]) && (j < L.n[1]);
+        for (int r = 0; r < CY; ++r)
+#pragma unroll
+            for (int e = 0; e < CX; ++e) act[r][e] = (i0 + e < L.n[0]) && (j0 + r < L.n[1]);
 
-        // q[e][m * NC + c]: column of cell e, plane it - 2G - U + m (before the shift of iteration it)
-        T q[CX][QL * NC];
+        // q[w][m * NC + c]: column w, plane it - 2G - U + m (before the shift of iteration it)
+        T q[NCOL][QL * NC];
 #pragma unroll
-        for (int e = 0; e < CX; ++e)
+        for (int w = 0; w < NCOL; ++w)
 #pragma unroll
-            for (int mm = 0; mm < QL * NC; ++mm) q[e][mm] = T(0);
+            for (int mm = 0; mm < QL * NC; ++mm) q[w][mm] = T(0);
 
-        const T* in_col = in + L.index(i0, j, 0, 0); // global fallback: cell 0's column at z = 0
+        const T* in_col = in + L.index(i0, j0, 0, 0); // global fallback: cell (i0, j0)'s column at z = 0
         const long long plane = L.px * L.py;
 
         // Prologue: planes 0 .. 2G-1 (the lower halo and the first G centre planes) into the
@@ -427,12 +440,14 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
             if (ok) {
                 const T* pl = reinterpret_cast<const T*>(smem_raw + pos.s * SSLOT) + coff;
 #pragma unroll
-                for (int c = 0; c < NC; ++c) {
-                    T v[CX];
-                    lds<CX>(pl + c * PNS, v);
+                for (int r = 0; r < CY; ++r)
 #pragma unroll
-                    for (int e = 0; e < CX; ++e) q[e][(p + U) * NC + c] = v[e];
-                }
+                    for (int c = 0; c < NC; ++c) {
+                        T v[CX];
+                        lds<CX>(pl + r * BX + c * PNS, v);
+#pragma unroll
+                        for (int e = 0; e < CX; ++e) q[r * CX + e][(Cfg::ROT ? p : p + U) * NC + c] = v[e];
+                    }
                 if (p < G || p >= NP - G) {
                     __syncwarp();
                     if (lane == 0) ptx::mbar_arrive(&empty[pos.s]);
@@ -444,7 +459,14 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
 
         // Main loop: U planes per iteration. Cell (e, u) has centre plane it - G + u, i.e.
         // z = z0 - 2G + it + u, and exists while it + u < NP; its queue window is q[e][u ...].
-        for (int it = 2 * G; it < NP; it += U) {
+        // Circular queue (ROT): plane p lives in slot p % QL, the loop is unrolled QL times and
+        // unrolled copy k (it = 2G + k mod QL) finds offset dk of its centre in slot (G + dk + k) % QL.
+        constexpr int KU = Cfg::ROT ? QL : 1;
+        for (int base = 2 * G; base < NP && ok; base += KU * U)
+#pragma unroll
+        for (int k = 0; k < KU; ++k) {
+            const int it = base + k * U;
+            if (Cfg::ROT && it >= NP) break;
             int su[U], scu[U], sku[U];
             {
                 RingPos pp = pos, cp = cpos, kp = kpos;
@@ -460,56 +482,82 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
                 }
             }
             if (!ok) break;
+            if constexpr (!Cfg::ROT) {
 #pragma unroll
-            for (int e = 0; e < CX; ++e)
+                for (int w = 0; w < NCOL; ++w)
 #pragma unroll
-                for (int mm = 0; mm < 2 * G * NC; ++mm) q[e][mm] = q[e][mm + U * NC];
+                    for (int mm = 0; mm < 2 * G * NC; ++mm) q[w][mm] = q[w][mm + U * NC];
+            }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 if (U == 1 || it + u < NP) {
                     const T* pl = reinterpret_cast<const T*>(smem_raw + su[u] * SSLOT) + coff;
+                    const int qs = Cfg::ROT ? (k + 2 * G) % QL : 2 * G + u; // queue slot of the newest plane
 #pragma unroll
-                    for (int c = 0; c < NC; ++c) {
-                        T v[CX];
-                        lds<CX>(pl + c * PNS, v);
+                    for (int r = 0; r < CY; ++r)
 #pragma unroll
-                        for (int e = 0; e < CX; ++e) q[e][(2 * G + u) * NC + c] = v[e];
-                    }
+                        for (int c = 0; c < NC; ++c) {
+                            T v[CX];
+                            lds<CX>(pl + r * BX + c * PNS, v);
+#pragma unroll
+                            for (int e = 0; e < CX; ++e) q[r * CX + e][qs * NC + c] = v[e];
+                        }
                 }
             }
 
             // all cells' stage values first, then the epilogues (their global stores would
             // otherwise stand between the shared-memory taps of neighbouring cells)
-            T kv[U][CX][NC];
+            T kv[U][CY][CX][NC];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int z = b.z0 - 2 * G + it + u;
                 const T* ctr = reinterpret_cast<const T*>(smem_raw + scu[u] * SSLOT) + coff;
 #pragma unroll
-                for (int e = 0; e < CX; ++e) {
+                for (int r = 0; r < CY; ++r)
 #pragma unroll
-                    for (int c = 0; c < NC; ++c) kv[u][e][c] = T(0);
-                    if ((U == 1 || it + u < NP) && act[e]) {
-                        amrex::StencilView<T> view{ctr + e,         q[e] + u * NC, in_col + e + z * plane, L.px, plane,
-                                                   L.comp_stride(), i0 + e,        j, z, BX, PNS, G, NC};
-                        amrex::Array4<const T> arr = make_array4<const T>(in, L);
-                        arr.view = &view;
-                        typename RHS::Workspace ws{};
-                        const amrex::IntVect idx{i0 + e, j, z};
-                        eval_components(f, kv[u][e], idx, time, arr, geom, ws, std::make_integer_sequence<int, NC>{});
+                    for (int e = 0; e < CX; ++e) {
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) kv[u][r][e][c] = T(0);
+                        if ((U == 1 || it + u < NP) && act[r][e]) {
+                            amrex::StencilView<T> view{ctr + r * BX + e,
+                                                       q[r * CX + e] + (Cfg::ROT ? 0 : u * NC),
+                                                       in_col + r * L.px + e + z * plane,
+                                                       L.px,
+                                                       plane,
+                                                       L.comp_stride(),
+                                                       i0 + e,
+                                                       j0 + r,
+                                                       z,
+                                                       BX,
+                                                       PNS,
+                                                       G,
+                                                       NC,
+                                                       Cfg::ROT ? k : 0,
+                                                       Cfg::ROT ? QL : 0};
+                            amrex::Array4<const T> arr = make_array4<const T>(in, L);
+                            arr.view = &view;
+                            typename RHS::Workspace ws{};
+                            const amrex::IntVect idx{i0 + e, j0 + r, z};
+                            eval_components(f, kv[u][r][e], idx, time, arr, geom, ws,
+                                            std::make_integer_sequence<int, NC>{});
+                        }
                     }
-                }
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 if (U == 1 || it + u < NP) {
                     const int z = b.z0 - 2 * G + it + u;
                     const unsigned char* cslot = cring + sku[u] * CSLOT;
-                    const CentreOps<C0, C1> co{reinterpret_cast<const C0*>(cslot + RingT::C0_OFF) + cc,
-                                               reinterpret_cast<const C1*>(cslot + RingT::C1_OFF) + cc, CPS};
-                    Epi::template apply<T, NC, CX>(epl, kv[u], act,
-                                                   reinterpret_cast<const T*>(smem_raw + scu[u] * SSLOT) + coff,
-                                                   PNS, i0, j, z, co);
+#pragma unroll
+                    for (int r = 0; r < CY; ++r) {
+                        const CentreOps<C0, C1> co{reinterpret_cast<const C0*>(cslot + RingT::C0_OFF) + cc + r * TX,
+                                                   reinterpret_cast<const C1*>(cslot + RingT::C1_OFF) + cc + r * TX,
+                                                   CPS};
+                        Epi::template apply<T, NC, CX>(
+                            epl, kv[u][r], act[r],
+                            reinterpret_cast<const T*>(smem_raw + scu[u] * SSLOT) + coff + r * BX, PNS, i0, j0 + r, z,
+                            co);
+                    }
                 }
             }
             __syncwarp();
@@ -760,14 +808,14 @@ struct LaunchShape {
     int nchunks = 0, zchunk = 0;
 };
 
-/// z-major grid: tiles of 32 x ty cells, the z extent split into `nchunks` chunks so that the
+/// z-major grid: tiles of TX x ty CY cells, the z extent split into `nchunks` chunks so that the
 /// grid fills the resident CTA slots without chunks shorter than 4G planes (each chunk pays a
 /// 2G-plane warm-up).
 template <class Cfg> LaunchShape make_shape(const Layout& L, int slots, int ty, int nchunks = 0) {
     LaunchShape s;
     s.ty = ty;
     s.ntx = (L.n[0] + Cfg::TX - 1) / Cfg::TX;
-    s.nty = (L.n[1] + ty - 1) / ty;
+    s.nty = (L.n[1] + ty * Cfg::CY - 1) / (ty * Cfg::CY);
     const int ntiles = s.ntx * s.nty;
     if (nchunks <= 0) {
         nchunks = slots / ntiles;
@@ -824,17 +872,17 @@ template <class Cfg, class RHS, class Epi> struct StageLauncher {
         if (ty <= 0 || ty > Cfg::TYMAX) ty = choose_ty<Cfg>(L, slots);
         return make_shape<Cfg>(L, slots, ty, nchunks);
     }
-    /// The TMA box of the stencil input for a launch shape: (TX + 2 XH) x (ty + 2G).
+    /// The TMA box of the stencil input for a launch shape: (TX + 2 XH) x (ty CY + 2G).
     static int box_x() { return Cfg::BX; }
-    static int box_y(const LaunchShape& s) { return s.ty + 2 * Cfg::G; }
-    /// Centre-operand descriptors (box TX x ty) from `map(base, layout, dtype, box_x, box_y)`,
+    static int box_y(const LaunchShape& s) { return s.ty * Cfg::CY + 2 * Cfg::G; }
+    /// Centre-operand descriptors (box TX x ty CY) from `map(base, layout, dtype, box_x, box_y)`,
     /// which returns a const CUtensorMap&.
     template <class MapFn>
     static CentreMaps centre_maps(MapFn&& map, const typename Epi::Params& ep, const LaunchShape& s) {
         CentreMaps cm{};
         for (int k = 0; k < Epi::kCentre; ++k) {
             const CentreSrc src = Epi::centre_src(ep, k);
-            cm.map[k] = map(src.base, src.L, src.dtype, Cfg::TX, s.ty);
+            cm.map[k] = map(src.base, src.L, src.dtype, Cfg::TX, s.ty * Cfg::CY);
             cm.x[k] = src.L.xoff;
             cm.y[k] = src.L.g;
             cm.z[k] = src.L.g;

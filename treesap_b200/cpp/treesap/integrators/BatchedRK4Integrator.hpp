@@ -393,7 +393,7 @@ class BatchedRK4Integrator {
             const auto& in = insts[i];
             int zc = zchunk_ > 0 ? zchunk_ : in.n[2];
             for (int z0 = 0; z0 < in.n[2]; z0 += zc)
-                for (int y0 = 0; y0 < in.n[1]; y0 += ty)
+                for (int y0 = 0; y0 < in.n[1]; y0 += ty * Cfg::CY)
                     for (int x0 = 0; x0 < in.n[0]; x0 += Cfg::TX)
                         v.push_back({i, x0, y0, z0, std::min(in.n[2], z0 + zc)});
         }
@@ -420,12 +420,12 @@ class BatchedRK4Integrator {
             typename Epi::Params ep = make(i, input, L);
             Entry& e = h.p[i];
             const ts_field_layout cl = L.to_c(dtype);
-            treesap_b200::ts_check(ts_field_tensor_map(&cl, input, Cfg::BX, ty + 2 * Cfg::G, &e.tmap), ctx,
+            treesap_b200::ts_check(ts_field_tensor_map(&cl, input, Cfg::BX, ty * Cfg::CY + 2 * Cfg::G, &e.tmap), ctx,
                                    "ts_field_tensor_map");
             for (int k = 0; k < Epi::kCentre; ++k) {
                 const treesap_b200::CentreSrc c = Epi::centre_src(ep, k);
                 const ts_field_layout cc = c.L.to_c(c.dtype);
-                treesap_b200::ts_check(ts_field_tensor_map(&cc, c.base, Cfg::TX, ty, &e.cmaps.map[k]), ctx,
+                treesap_b200::ts_check(ts_field_tensor_map(&cc, c.base, Cfg::TX, ty * Cfg::CY, &e.cmaps.map[k]), ctx,
                                        "ts_field_tensor_map");
                 e.cmaps.x[k] = c.L.xoff;
                 e.cmaps.y[k] = c.L.g;
