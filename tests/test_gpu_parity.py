@@ -123,6 +123,24 @@ def test_variable_speed_matches_oracle(ctx, port_oracle):
     assert relerr(gpu, cpu) <= TOL_F64
 
 
+@pytest.mark.parametrize("ngrow,periodic", [(2, (1, 1, 1)), (4, (0, 0, 0)), (3, (1, 0, 1))])
+def test_fp32_stage_without_decorators(ctx, ngrow, periodic):
+    """FP32-stage RK4 of the undecorated wave model (no Kreiss-Oliger, no layer): the right-hand
+    side is its own linear part, so stages 0 and 1 run the same functor type."""
+    bc = TS_BC_NOOP if all(periodic) else TS_BC_DIRICHLET
+    mk = lambda p: wave_desc((40, 36, 32), ngrow, periodic=periodic, bc=bc, precision=p, dt=0.25 / 40)
+    pul = c2_pulses(1, 4)
+    out = {}
+    for p in (TS_F64, TS_F32_STAGE):
+        it = Integrator(ctx, mk(p))
+        it.initialise(TS_INIT_GAUSSIAN, pul)
+        it.step(40)
+        out[p] = it.get_state()
+    ctx.sync()
+    assert np.abs(out[TS_F64]).max() > 0.1
+    assert relerr(out[TS_F32_STAGE], out[TS_F64]) <= 1e-6
+
+
 @pytest.mark.parametrize("bcmode", ["periodic", "abl"])
 def test_fp32_stage_error_vs_fp64(ctx, bcmode):
     """FP32-stage RK4 vs FP64 GPU path: max-norm relative error <= 1e-6 after 200 steps."""

@@ -896,11 +896,17 @@ template <class Cfg, class RHS, class Epi> struct StageLauncher {
         sp.ty = s.ty;
         sp.zchunk = s.zchunk;
         const int threads = 32 * s.ty + 32;
-        stage_kernel<Cfg, RHS, Epi><<<s.grid, threads, RingT::SMEM, stream>>>(tmap, cmaps, sp, rhs, ep);
-        const cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess)
+        // Launched through the registered entry point rather than <<< >>>: for some
+        // instantiations (template arguments spelled through class-member aliases) the
+        // front end's generated launch wrapper resolved to its unspecialised fallback, which
+        // launches nothing and reports cudaErrorInvalidDeviceFunction.
+        void* args[] = {const_cast<CUtensorMap*>(&tmap), const_cast<CentreMaps*>(&cmaps), &sp,
+                        const_cast<RHS*>(&rhs), const_cast<typename Epi::Params*>(&ep)};
+        const cudaError_t err = cudaLaunchKernel(reinterpret_cast<const void*>(kernel()), dim3(s.grid), dim3(threads),
+                                                 args, size_t(RingT::SMEM), stream);
+        if (err != cudaSuccess)
             throw std::runtime_error(std::string("stage_kernel launch (") + __PRETTY_FUNCTION__ +
-                                     "): " + cudaGetErrorString(e));
+                                     "): " + cudaGetErrorString(err));
     }
 };
 

@@ -326,9 +326,14 @@ class BatchedRK4Integrator {
             int g = grid(sms);
             if (g > items.n) g = items.n;
             if (g < 1) return;
-            treesap_b200::batch_stage_kernel<Cfg, R, Epi>
-                <<<g, 32 * ty + 32, RingT::SMEM, s>>>(entries.p, items.p, items.n, ty, err);
-            treesap_b200::cuda_check(cudaGetLastError(), "batch_stage_kernel launch");
+            // through the registered entry point, like StageLauncher::launch
+            const Entry* e = entries.p;
+            const treesap_b200::ItemBox* it = items.p;
+            int n = int(items.n);
+            void* args[] = {&e, &it, &n, &ty, &err};
+            treesap_b200::cuda_check(cudaLaunchKernel(reinterpret_cast<const void*>(kernel()), dim3(g),
+                                                      dim3(32 * ty + 32), args, size_t(RingT::SMEM), s),
+                                     "batch_stage_kernel launch");
         }
     };
 
