@@ -152,9 +152,13 @@ template <class U> struct StencilView {
     int qg, qnc;     // register queue half-depth and component count
     int qrot = 0;    // circular queue (qlen > 0): offset k + dk sits in slot (dk + qg + qrot) % qlen
     int qlen = 0;
+    const U* xw = nullptr; // registers: the centre row around the cell, [qnc][xwn], offset di at xw0 + di
+    int xwn = 0, xw0 = 0;
 
     AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE const U& at(int i, int j, int k, int n) const {
         const int di = i - ci, dj = j - cj, dk = k - ck;
+        if (xw != nullptr && dk == 0 && dj == 0 && xw0 + di >= 0 && xw0 + di < xwn && n < qnc)
+            return xw[n * xwn + xw0 + di];
         if (dk == 0) return plane[n * pns + dj * pjs + di];
         if (di == 0 && dj == 0 && dk >= -qg && dk <= qg && n < qnc) {
             const int m = dk + qg + qrot;

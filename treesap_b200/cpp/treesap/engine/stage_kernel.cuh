@@ -215,6 +215,17 @@ __device__ __forceinline__ void eval_components(const RHS& f, T (&kv)[NC], const
     ((kv[C] = static_cast<T>(f.template operator()<C>(idx, time, arr, geom, ws))), ...);
 }
 
+/// The stage values of one cell: the RHS on an Array4 whose accesses the view resolves.
+template <class RHS, class T, int NC>
+__device__ __forceinline__ void eval_cell(const RHS& f, T (&kv)[NC], const amrex::StencilView<T>& view, const T* in,
+                                          const Layout& L, const amrex::IntVect& idx, double time,
+                                          const amrex::GeometryData& geom) {
+    amrex::Array4<const T> arr = make_array4<const T>(in, L);
+    arr.view = &view;
+    typename RHS::Workspace ws{};
+    eval_components(f, kv, idx, time, arr, geom, ws, std::make_integer_sequence<int, NC>{});
+}
+
 /// One unit of work of a CTA: the tile at (x0, y0) of instance `inst`, planes z0 .. z1-1.
 struct ItemBox {
     int inst, x0, y0, z0, z1;
@@ -513,35 +524,67 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
                 const int z = b.z0 - 2 * G + it + u;
                 const T* ctr = reinterpret_cast<const T*>(smem_raw + scu[u] * SSLOT) + coff;
 #pragma unroll
-                for (int r = 0; r < CY; ++r)
+                for (int r = 0; r < CY; ++r) {
+                    // Two cells per thread: the centre row's x taps of both cells (offsets -GW ..
+                    // GW + 1 from cell 0, GW = G rounded up to even, GW <= XH) come from registers
+                    // filled with aligned vector loads; per-tap loads would be half misaligned
+                    // pairs, split into stride-2 scalar loads with two-way bank conflicts.
+                    constexpr int GW = (G + 1) / 2 * 2;
+                    constexpr int XWN = CX == 2 ? 2 * GW + 2 : 1;
+                    static_assert(CX == 1 || GW <= XH, "x window beyond the shared-memory halo");
+                    T xwin[NC][XWN];
+                    if constexpr (CX == 2) {
 #pragma unroll
-                    for (int e = 0; e < CX; ++e) {
+                        for (int c = 0; c < NC; ++c)
 #pragma unroll
-                        for (int c = 0; c < NC; ++c) kv[u][r][e][c] = T(0);
-                        if ((U == 1 || it + u < NP) && act[r][e]) {
-                            amrex::StencilView<T> view{ctr + r * BX + e,
-                                                       q[r * CX + e] + (Cfg::ROT ? 0 : u * NC),
-                                                       in_col + r * L.px + e + z * plane,
-                                                       L.px,
-                                                       plane,
-                                                       L.comp_stride(),
-                                                       i0 + e,
-                                                       j0 + r,
-                                                       z,
-                                                       BX,
-                                                       PNS,
-                                                       G,
-                                                       NC,
-                                                       Cfg::ROT ? k : 0,
-                                                       Cfg::ROT ? QL : 0};
-                            amrex::Array4<const T> arr = make_array4<const T>(in, L);
-                            arr.view = &view;
-                            typename RHS::Workspace ws{};
-                            const amrex::IntVect idx{i0 + e, j0 + r, z};
-                            eval_components(f, kv[u][r][e], idx, time, arr, geom, ws,
-                                            std::make_integer_sequence<int, NC>{});
+                            for (int h = 0; h < XWN / 2; ++h) {
+                                T v[2];
+                                lds<2>(ctr + r * BX + c * PNS - GW + 2 * h, v);
+                                xwin[c][2 * h] = v[0];
+                                xwin[c][2 * h + 1] = v[1];
+                            }
+                    }
+                    amrex::StencilView<T> view[CX];
+#pragma unroll
+                    for (int e = 0; e < CX; ++e)
+                        view[e] = amrex::StencilView<T>{ctr + r * BX + e,
+                                                        q[r * CX + e] + (Cfg::ROT ? 0 : u * NC),
+                                                        in_col + r * L.px + e + z * plane,
+                                                        L.px,
+                                                        plane,
+                                                        L.comp_stride(),
+                                                        i0 + e,
+                                                        j0 + r,
+                                                        z,
+                                                        BX,
+                                                        PNS,
+                                                        G,
+                                                        NC,
+                                                        Cfg::ROT ? k : 0,
+                                                        Cfg::ROT ? QL : 0,
+                                                        CX == 2 ? &xwin[0][0] : nullptr,
+                                                        XWN,
+                                                        GW + e};
+                    bool whole = U == 1 || it + u < NP;
+#pragma unroll
+                    for (int e = 0; e < CX; ++e) whole = whole && act[r][e];
+                    if (CX > 1 && whole) {
+                        // every cell of the row exists: no per-cell branch, so the taps of
+                        // neighbouring cells can share vector loads
+#pragma unroll
+                        for (int e = 0; e < CX; ++e)
+                            eval_cell(f, kv[u][r][e], view[e], in, L, amrex::IntVect{i0 + e, j0 + r, z}, time, geom);
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < CX; ++e) {
+#pragma unroll
+                            for (int c = 0; c < NC; ++c) kv[u][r][e][c] = T(0);
+                            if ((U == 1 || it + u < NP) && act[r][e])
+                                eval_cell(f, kv[u][r][e], view[e], in, L, amrex::IntVect{i0 + e, j0 + r, z}, time,
+                                          geom);
                         }
                     }
+                }
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
