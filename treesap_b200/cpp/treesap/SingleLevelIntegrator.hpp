@@ -77,6 +77,8 @@ namespace detail {
 // components: it removes the per-plane queue shift (16 moves per FP64 component and cell at
 // ngrow 4) at the price of a plane loop unrolled 2 ngrow + 1 times. Measured at 256^3, ngrow 4:
 // FP64 stages 3-10% faster; FP32 stages (two cells per thread) 30% slower, so off for FP32.
+// One cell per thread only: with more, the unrolled loop outgrows full unrolling and the queue
+// index stops being a compile-time constant (the queue then lands in local memory).
 #ifndef TREESAP_B200_QROT_F64
 #define TREESAP_B200_QROT_F64 1
 #endif
@@ -91,7 +93,7 @@ template <typename T, int G, int NC> struct DefaultTile {
     using Spec = std::conditional_t<sizeof(T) == 8, TileSpec<TREESAP_B200_TILE_F64>, TileSpec<TREESAP_B200_TILE_F32>>;
     static constexpr bool kRot = (sizeof(T) == 8 ? TREESAP_B200_QROT_F64 : TREESAP_B200_QROT_F32) != 0 && NC <= 4;
     template <int CX, int TY, int P, int MINB, int U, int CY = 1>
-    using C = treesap_b200::TileCfg<CX, TY, G, NC, T, P, MINB, U, CY, kRot && U == 1>;
+    using C = treesap_b200::TileCfg<CX, TY, G, NC, T, P, MINB, U, CY, kRot && U == 1 && CX == 1 && CY == 1>;
     using Pref = C<Spec::CX, Spec::TY, Spec::P, Spec::MINB, Spec::U, Spec::CY>;
     using type = std::conditional_t<
         Pref::fits, Pref,
