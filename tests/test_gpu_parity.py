@@ -247,3 +247,60 @@ def test_tensor_fp32_stage_error_vs_fp64(ctx):
         out[p] = it.get_state()
     ctx.sync()
     assert relerr(out[TS_F32_STAGE], out[TS_F64]) <= 1e-6
+
+
+@pytest.mark.parametrize("n,ngrow,bcmode", [((4, 5, 4), 4, "periodic"), ((2, 6, 3), 2, "dirichlet"),
+                                             ((1, 1, 7), 1, "periodic"), ((4, 4, 9), 4, "dirichlet"),
+                                             ((3, 3, 3), 3, "periodic")])
+def test_extents_at_the_ghost_width(ctx, port_oracle, n, ngrow, bcmode):
+    """The smallest boxes the descriptor accepts (extents equal to the stencil half-width, so a
+    periodic image spans the whole box; one-cell directions at ngrow 1), far smaller than one
+    tile: RK4 FP64 against the oracle."""
+    kw = dict(ko=0.1, dt=0.05)
+    if bcmode == "periodic":
+        d = wave_desc(n, ngrow, periodic=(1, 1, 1), **kw)
+    else:
+        d = wave_desc(n, ngrow, periodic=(0, 1, 0), bc=TS_BC_DIRICHLET, bc_values=(0.25, -0.5), **kw)
+    state = smooth_state(d.shape(), seed=sum(n) + ngrow)
+    it = Integrator(ctx, d)
+    it.set_state(state)
+    it.step(3)
+    gpu = it.get_state()
+    ctx.sync()
+    cpu, _, _ = port_oracle.run(d, 3, state=state)
+    assert np.isfinite(gpu).all()
+    assert relerr(gpu, cpu) <= TOL_F64
+
+
+def test_extents_below_the_ghost_width_are_rejected(ctx):
+    from treesap_b200 import TSError
+
+    with pytest.raises(TSError, match="INVALID_ARGUMENT"):
+        Integrator(ctx, wave_desc((3, 8, 8), 4))
+
+
+@pytest.mark.parametrize("precision", [TS_F64, TS_F32_STAGE])
+def test_periodic_translation_equivariance_on_a_large_box(ctx, precision):
+    """Size-independent property at 512 x 256 x 192 (16 x-tiles of 32 cells, several z chunks):
+    on a periodic grid with uniform spacing the step commutes with a cyclic shift of the state,
+    bit for bit, because every cell runs the same arithmetic on the same neighbour values."""
+    n = (512, 256, 192)
+    d = wave_desc(n, 4, periodic=(1, 1, 1), ko=0.2, precision=precision, prob_hi=(2.0, 1.0, 0.75), dt=0.25 / 256)
+    rng = np.random.default_rng(3)
+    state = np.zeros(d.shape())
+    z, y, x = np.meshgrid(*(np.arange(m) / m for m in n[::-1]), indexing="ij")
+    for c in range(2):
+        for _ in range(3):
+            k = rng.integers(-3, 4, 3)
+            state[c] += rng.normal() * np.cos(2 * np.pi * (k[0] * x + k[1] * y + k[2] * z) + rng.uniform(0, 6.28))
+    shift = (5, -3, 7)  # cells along z, y, x
+    outs = []
+    for s in (state, np.roll(state, shift, axis=(1, 2, 3))):
+        it = Integrator(ctx, d)
+        it.set_state(s)
+        it.step(2)
+        outs.append(it.get_state())
+        it.close()
+    ctx.sync()
+    assert np.abs(outs[0]).max() > 0.1
+    assert np.array_equal(np.roll(outs[0], shift, axis=(1, 2, 3)), outs[1])
