@@ -39,6 +39,37 @@ AMREX_GPU_HOST_DEVICE inline GhostCount ghost_count(const Layout& L) {
 AMREX_GPU_HOST_DEVICE inline void ghost_coords(const Layout& L, long long t, int& i, int& j, int& k) {
     const GhostCount gc = ghost_count(L);
     const int g = L.g, n0 = L.n[0], n1 = L.n[1], n2 = L.n[2];
+    if (gc.total() < (1LL << 31)) {
+        // the same enumeration in 32-bit arithmetic (64-bit divisions cost several times more)
+        const unsigned row = unsigned(n0 + 2 * g), twog = unsigned(2 * g);
+        unsigned u = unsigned(t);
+        if (u < unsigned(gc.z)) {
+            const unsigned q = u / row, rows = unsigned(n1 + 2 * g);
+            i = int(u - q * row) - g;
+            const unsigned kk = q / rows;
+            j = int(q - kk * rows) - g;
+            k = int(kk) < g ? int(kk) - g : n2 + (int(kk) - g);
+            return;
+        }
+        u -= unsigned(gc.z);
+        if (u < unsigned(gc.y)) {
+            const unsigned q = u / row;
+            i = int(u - q * row) - g;
+            const unsigned kq = q / twog;
+            const int jj = int(q - kq * twog);
+            k = int(kq);
+            j = jj < g ? jj - g : n1 + (jj - g);
+            return;
+        }
+        u -= unsigned(gc.y);
+        const unsigned q = u / twog;
+        const int ii = int(u - q * twog);
+        const unsigned kq = q / unsigned(n1);
+        k = int(kq);
+        j = int(q - kq * unsigned(n1));
+        i = ii < g ? ii - g : n0 + (ii - g);
+        return;
+    }
     if (t < gc.z) {
         const long long row = n0 + 2 * g, plane = row * (n1 + 2 * g);
         const int kk = int(t / plane);

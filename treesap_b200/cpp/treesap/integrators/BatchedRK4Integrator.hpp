@@ -150,7 +150,14 @@ class BatchedRK4Integrator {
     /// Tile rows and z-range length of the work items (0 = automatic); invalidates the plans.
     void set_launch_shape(int rows, int zchunk) {
         rows_ = rows;
+        rows32_ = 0;
         zchunk_ = zchunk;
+        drop_graphs();
+        free_plans();
+    }
+    /// Tile rows of the FP32-input stages of the FP32-stage form (0 = those of set_launch_shape).
+    void set_fp32_rows(int rows) {
+        rows32_ = rows;
         drop_graphs();
         free_plans();
     }
@@ -246,6 +253,43 @@ class BatchedRK4Integrator {
             }
         }
         set_launch_shape(best_shape.first, best_shape.second);
+        if constexpr (F32Stage) {
+            // the FP32-input stages (two cells per thread) may prefer other tile rows than the
+            // FP64-input ones: refine them with the FP64 rows and z ranges fixed
+            int best32 = 0;
+            for (int ty = Tile32::TYMAX; ty >= 2; --ty) {
+                if (ty == best_shape.first) continue;
+                set_fp32_rows(ty);
+                step(1);
+                step(trial_steps);
+                treesap_b200::cuda_check(cudaStreamSynchronize(stream()), "cudaStreamSynchronize");
+                const double ms = last_step_timing().first;
+                if (ms < best) {
+                    best = ms;
+                    best32 = ty;
+                }
+            }
+            set_fp32_rows(best32);
+            // and the FP64-input stages with those FP32 rows
+            const int r32 = best32 > 0 ? best32 : best_shape.first;
+            int best64 = best_shape.first;
+            for (int ty = Tile64::TYMAX; ty >= 2; --ty) {
+                if (ty == best_shape.first) continue;
+                set_launch_shape(ty, best_shape.second);
+                set_fp32_rows(r32);
+                step(1);
+                step(trial_steps);
+                treesap_b200::cuda_check(cudaStreamSynchronize(stream()), "cudaStreamSynchronize");
+                const double ms = last_step_timing().first;
+                if (ms < best) {
+                    best = ms;
+                    best64 = ty;
+                }
+            }
+            best_shape.first = best64;
+            set_launch_shape(best64, best_shape.second);
+            set_fp32_rows(r32);
+        }
         // restore the states into the saved parity's buffers, ghost cells included
         nsteps_done = saved_steps;
         fills_done[0] = fills_done[1] = false;
@@ -387,6 +431,8 @@ class BatchedRK4Integrator {
     }
 
     template <class Cfg> int rows_for() const {
+        if constexpr (std::is_same_v<Cfg, Tile32> && !std::is_same_v<Tile32, Tile64>)
+            if (rows32_ > 0 && rows32_ <= Cfg::TYMAX) return rows32_;
         if (rows_ > 0 && rows_ <= Cfg::TYMAX) return rows_;
         return Cfg::TYMAX;
     }
@@ -659,7 +705,7 @@ class BatchedRK4Integrator {
     Plan plan[2];
     DevArray<treesap_b200::ItemBox> items64, items32;
     int ty_[2] = {0, 0};
-    int rows_ = 0, zchunk_ = 0;
+    int rows_ = 0, rows32_ = 0, zchunk_ = 0;
     bool plans_ready = false;
     bool graphs_on = false;
     bool fills_done[2] = {false, false};
