@@ -1,7 +1,7 @@
 """Stage-kernel tile configurations agree bitwise.
 
-The tiling (cells per thread along x, rows per consumer warp, tile height, circular or
-shifted register queue, prefetch depth) only changes which thread evaluates which cell and
+The tiling (cells per thread along x, rows per consumer warp, tile height, circular,
+shifted or no register queue, prefetch depth) only changes which thread evaluates which cell and
 where the operands wait, never the per-cell arithmetic. tests/cpp/tile_variant_driver.cu is
 built once per configuration (compile-time switches of the front end) and every build must
 write the same bytes for the FP64 and the FP32-stage forms on a ragged 72 x 45 x 37 box
@@ -25,6 +25,7 @@ VARIANTS = {
     "circular FP32 queue": ["-DTREESAP_B200_QROT_F32=1"],
     "two rows per warp": ["-DTREESAP_B200_TILE_F64=2105421", "-DTREESAP_B200_TILE_F32=2105421"],
     "two FP64 cells per thread, short prefetch": ["-DTREESAP_B200_TILE_F64=204221", "-DTREESAP_B200_TILE_F32=103221"],
+    "z taps from global memory": ["-DTREESAP_B200_QUEUE_MAX_COMPONENTS=0"],
 }
 
 

@@ -89,11 +89,29 @@ template <int code> struct TileSpec {
     static constexpr int CY = code / 1000000 > 0 ? code / 1000000 : 1, CX = code / 100000 % 10,
                          TY = code / 1000 % 100, P = code / 100 % 10, MINB = code / 10 % 10, U = code % 10;
 };
+// Models of more than kQueueMaxComponents components stream only the centre planes and read
+// their z taps from global memory (TileCfg::ZQ = false): a register queue of 2 ngrow + 1 planes
+// of every component does not fit the registers (12 FP64 components at ngrow 3: 168 registers
+// of queue alone, kilobytes of spills). Their tiles: TREESAP_B200_TILE_MANY_F64 / _F32.
+#ifndef TREESAP_B200_TILE_MANY_F64
+#define TREESAP_B200_TILE_MANY_F64 103121
+#endif
+#ifndef TREESAP_B200_TILE_MANY_F32
+#define TREESAP_B200_TILE_MANY_F32 107121
+#endif
+#ifndef TREESAP_B200_QUEUE_MAX_COMPONENTS
+#define TREESAP_B200_QUEUE_MAX_COMPONENTS 4
+#endif
+constexpr int kQueueMaxComponents = TREESAP_B200_QUEUE_MAX_COMPONENTS;
 template <typename T, int G, int NC> struct DefaultTile {
-    using Spec = std::conditional_t<sizeof(T) == 8, TileSpec<TREESAP_B200_TILE_F64>, TileSpec<TREESAP_B200_TILE_F32>>;
-    static constexpr bool kRot = (sizeof(T) == 8 ? TREESAP_B200_QROT_F64 : TREESAP_B200_QROT_F32) != 0 && NC <= 4;
+    static constexpr bool kQueue = NC <= kQueueMaxComponents;
+    using Spec = std::conditional_t<
+        kQueue,
+        std::conditional_t<sizeof(T) == 8, TileSpec<TREESAP_B200_TILE_F64>, TileSpec<TREESAP_B200_TILE_F32>>,
+        std::conditional_t<sizeof(T) == 8, TileSpec<TREESAP_B200_TILE_MANY_F64>, TileSpec<TREESAP_B200_TILE_MANY_F32>>>;
+    static constexpr bool kRot = (sizeof(T) == 8 ? TREESAP_B200_QROT_F64 : TREESAP_B200_QROT_F32) != 0 && kQueue;
     template <int CX, int TY, int P, int MINB, int U, int CY = 1>
-    using C = treesap_b200::TileCfg<CX, TY, G, NC, T, P, MINB, U, CY, kRot && U == 1 && CX == 1 && CY == 1>;
+    using C = treesap_b200::TileCfg<CX, TY, G, NC, T, P, MINB, U, CY, kRot && U == 1 && CX == 1 && CY == 1, kQueue>;
     using Pref = C<Spec::CX, Spec::TY, Spec::P, Spec::MINB, Spec::U, Spec::CY>;
     using type = std::conditional_t<
         Pref::fits, Pref,

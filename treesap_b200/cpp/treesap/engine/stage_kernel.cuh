@@ -59,10 +59,16 @@ constexpr int align128(int b) { return (b + 127) / 128 * 128; }
 /// is ty * CY rows high), ghost width G, NC components of type T, up to P planes of prefetch,
 /// MINB resident CTAs per SM, U planes per iteration of the plane loop.
 template <int CX_, int TYMAX_, int G_, int NC_, typename T_, int P_ = 2, int MINB_ = 2, int U_ = 1, int CY_ = 1,
-          bool ROT_ = false>
+          bool ROT_ = false, bool ZQ_ = true>
 struct TileCfg {
     using T = T_;
     static constexpr int CX = CX_, TX = 32 * CX_, TYMAX = TYMAX_, G = G_, NC = NC_, P = P_, U = U_, CY = CY_;
+    /// ZQ: z taps at the cell's column from a register queue of 2G + U planes fed by a ring that
+    /// also streams the G halo planes above and below; !ZQ (many components, whose queue would
+    /// not fit the registers): the ring streams only the centre planes and every tap off the
+    /// centre plane is a global load (L1/L2).
+    static constexpr bool ZQ = ZQ_;
+    static constexpr int ZH = ZQ_ ? G_ : 0; // halo planes streamed below and above a z range
     /// Circular register queue: the plane loop is unrolled by the queue depth 2G + 1 so that
     /// every plane keeps its register slot (plane % (2G + 1)) instead of being shifted.
     static constexpr bool ROT = ROT_;
@@ -78,10 +84,10 @@ struct TileCfg {
     /// Dynamic shared memory per CTA when MIN_BLOCKS CTAs share an SM (228 KB per SM with 1 KB
     /// reserved per CTA; at most 227 KB for one CTA).
     static constexpr int SMEM_BUDGET = MINB_ == 1 ? 232448 : 233472 / MINB_ - 1024;
-    /// Shared memory of a stencil ring of G + U + p slots and a centre-operand ring of U + p
+    /// Shared memory of a stencil ring of ZH + U + p slots and a centre-operand ring of U + p
     /// slots of `cslot` bytes (none when cslot = 0), with their mbarriers.
     static constexpr int smem_for(int p, int cslot) {
-        return (G + U + p) * (STENCIL_BYTES + 16) + (cslot > 0 ? (U + p) * (cslot + 8) : 0);
+        return (ZH + U + p) * (STENCIL_BYTES + 16) + (cslot > 0 ? (U + p) * (cslot + 8) : 0);
     }
     /// Usable when even two FP64 centre-operand fields fit with one plane of prefetch.
     static constexpr bool fits = smem_for(1, 2 * align128(CBOX * 8)) <= SMEM_BUDGET;
@@ -89,6 +95,7 @@ struct TileCfg {
     static_assert(U == 1 || U == 2, "one or two planes per iteration");
     static_assert(CY >= 1 && CY <= 4, "one to four rows per consumer warp");
     static_assert(!ROT || U == 1, "the circular queue takes one plane per iteration");
+    static_assert(ZQ || (U == 1 && !ROT), "without the register queue: one plane per iteration, no rotation");
     static_assert(BX <= 256 && BYMAX <= 256 && NC <= 256, "TMA box dimensions are limited to 256");
     static_assert(THREADS <= 1024, "too many threads");
 };
@@ -116,7 +123,7 @@ template <class Cfg, class Epi> struct Ring {
         while (p > 1 && Cfg::smem_for(p, CSLOT) > Cfg::SMEM_BUDGET) --p;
         return p;
     }();
-    static constexpr int R = Cfg::G + Cfg::U + P;
+    static constexpr int R = Cfg::ZH + Cfg::U + P;
     static constexpr int RC = NCEN > 0 ? Cfg::U + P : 0;
     static constexpr int CRING_OFF = R * SSLOT;             // centre ring
     static constexpr int BAR_OFF = CRING_OFF + RC * CSLOT;  // full[R], empty[R], cempty[RC]
@@ -301,7 +308,7 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
     using RingT = Ring<Cfg, Epi>;
     using C0 = typename RingT::C0;
     using C1 = typename RingT::C1;
-    constexpr int G = Cfg::G, NC = Cfg::NC, TX = Cfg::TX, BX = Cfg::BX, XH = Cfg::XH;
+    constexpr int G = Cfg::G, NC = Cfg::NC, TX = Cfg::TX, BX = Cfg::BX, XH = Cfg::XH, ZH = Cfg::ZH;
     constexpr int R = RingT::R, RC = RingT::RC, SSLOT = RingT::SSLOT, CSLOT = RingT::CSLOT, NCEN = RingT::NCEN;
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -358,23 +365,23 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
                     cy[k] = cm.y[k];
                     cz[k] = cm.z[k];
                 }
-                const int NP = (b.z1 - b.z0) + 2 * G; // planes z0 - G .. z1 - 1 + G
+                const int NP = (b.z1 - b.z0) + 2 * ZH; // planes z0 - ZH .. z1 - 1 + ZH
                 for (int q = 0; q < NP; ++q, ++t) {
                     if (t >= R && !ptx::mbar_wait(&empty[ps.s], ps.ph ^ 1u, err)) {
                         ok = false;
                         break;
                     }
-                    const bool centre = NCEN > 0 && q >= 2 * G;
+                    const bool centre = NCEN > 0 && q >= 2 * ZH;
                     if (centre && tc >= RC && !ptx::mbar_wait(&cempty[pc.s], pc.ph ^ 1u, err)) {
                         ok = false;
                         break;
                     }
                     ptx::mbar_arrive_expect_tx(&full[ps.s], bytes + (centre ? cbytes : 0u));
                     // storage coordinates: x = x0 - XH + xoff (= x0), y = y0 - G + g (= y0), z = z0 - G + q + g
-                    ptx::tma_load_4d(smem_raw + ps.s * SSLOT, tmap, b.x0, b.y0, b.z0 + q, 0, &full[ps.s]);
+                    ptx::tma_load_4d(smem_raw + ps.s * SSLOT, tmap, b.x0, b.y0, b.z0 + q + (G - ZH), 0, &full[ps.s]);
                     if constexpr (NCEN > 0) {
                         if (centre) {
-                            const int zc = b.z0 - 2 * G + q;
+                            const int zc = b.z0 - 2 * ZH + q;
                             unsigned char* cs = cring + pc.s * CSLOT;
                             ptx::tma_load_4d(cs + RingT::C0_OFF, &cm.map[0], b.x0 + cx[0], b.y0 + cy[0], zc + cz[0], 0,
                                              &full[ps.s]);
@@ -400,7 +407,7 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
 
     // -------------------------------------------------------------------- consumer warps
     constexpr int CX = Cfg::CX, U = Cfg::U;
-    constexpr int QL = 2 * G + U;  // register queue depth (planes)
+    constexpr int QL = 2 * ZH + U; // register queue depth (planes)
     constexpr int NCOL = CY * CX;  // columns (cells per plane) of a thread: column r CX + e is cell (i0 + e, j0 + r)
     const int tx = lane, ty = warp;
     const int coff = (CY * ty + G) * BX + (CX * tx + XH); // cell (i0, j0)'s centre inside the stencil plane (row r: + r BX)
@@ -422,7 +429,7 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
         const T* const in = spr.in;
         const typename Epi::Params epl = src.epi(b.inst);
 
-        const int NP = (b.z1 - b.z0) + 2 * G;
+        const int NP = (b.z1 - b.z0) + 2 * ZH;
         const int i0 = b.x0 + CX * tx, j0 = b.y0 + CY * ty; // this thread's cells: (i0 + e, j0 + r)
         bool act[CY][CX];
 #pragma unroll
@@ -443,10 +450,11 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
         // Prologue: planes 0 .. 2G-1 (the lower halo and the first G centre planes) into the
         // queue. Planes that are never centre planes (p < G, p >= NP - G) are released once
         // read; every other plane after its iteration as a centre plane.
-        RingPos cpos; // stencil slot of plane it - G
+        RingPos cpos; // stencil slot of plane it - ZH
+        if constexpr (ZH == 0) cpos = pos; // the newest plane is the centre plane
 #pragma unroll
-        for (int p = 0; p < 2 * G; ++p) {
-            if (p == G) cpos = pos;
+        for (int p = 0; p < 2 * ZH; ++p) {
+            if (p == ZH) cpos = pos;
             if (ok && !ptx::mbar_wait(&full[pos.s], pos.ph, err)) ok = false;
             if (ok) {
                 const T* pl = reinterpret_cast<const T*>(smem_raw + pos.s * SSLOT) + coff;
@@ -459,7 +467,7 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
 #pragma unroll
                         for (int e = 0; e < CX; ++e) q[r * CX + e][(Cfg::ROT ? p : p + U) * NC + c] = v[e];
                     }
-                if (p < G || p >= NP - G) {
+                if (p < ZH || p >= NP - ZH) {
                     __syncwarp();
                     if (lane == 0) ptx::mbar_arrive(&empty[pos.s]);
                 }
@@ -473,7 +481,7 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
         // Circular queue (ROT): plane p lives in slot p % QL, the loop is unrolled QL times and
         // unrolled copy k (it = 2G + k mod QL) finds offset dk of its centre in slot (G + dk + k) % QL.
         constexpr int KU = Cfg::ROT ? QL : 1;
-        for (int base = 2 * G; base < NP && ok; base += KU * U)
+        for (int base = 2 * ZH; base < NP && ok; base += KU * U)
 #pragma unroll
         for (int k = 0; k < KU; ++k) {
             const int it = base + k * U;
@@ -497,13 +505,13 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
 #pragma unroll
                 for (int w = 0; w < NCOL; ++w)
 #pragma unroll
-                    for (int mm = 0; mm < 2 * G * NC; ++mm) q[w][mm] = q[w][mm + U * NC];
+                    for (int mm = 0; mm < 2 * ZH * NC; ++mm) q[w][mm] = q[w][mm + U * NC];
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                if (U == 1 || it + u < NP) {
+                if (Cfg::ZQ && (U == 1 || it + u < NP)) {
                     const T* pl = reinterpret_cast<const T*>(smem_raw + su[u] * SSLOT) + coff;
-                    const int qs = Cfg::ROT ? (k + 2 * G) % QL : 2 * G + u; // queue slot of the newest plane
+                    const int qs = Cfg::ROT ? (k + 2 * ZH) % QL : 2 * ZH + u; // queue slot of the newest plane
 #pragma unroll
                     for (int r = 0; r < CY; ++r)
 #pragma unroll
@@ -521,7 +529,7 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
             T kv[U][CY][CX][NC];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const int z = b.z0 - 2 * G + it + u;
+                const int z = b.z0 - 2 * ZH + it + u;
                 const T* ctr = reinterpret_cast<const T*>(smem_raw + scu[u] * SSLOT) + coff;
 #pragma unroll
                 for (int r = 0; r < CY; ++r) {
@@ -558,8 +566,8 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
                                                         z,
                                                         BX,
                                                         PNS,
-                                                        G,
-                                                        NC,
+                                                        ZH,
+                                                        Cfg::ZQ ? NC : 0,
                                                         Cfg::ROT ? k : 0,
                                                         Cfg::ROT ? QL : 0,
                                                         CX == 2 ? &xwin[0][0] : nullptr,
@@ -589,7 +597,7 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 if (U == 1 || it + u < NP) {
-                    const int z = b.z0 - 2 * G + it + u;
+                    const int z = b.z0 - 2 * ZH + it + u;
                     const unsigned char* cslot = cring + sku[u] * CSLOT;
 #pragma unroll
                     for (int r = 0; r < CY; ++r) {
@@ -610,7 +618,7 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
                     if (U == 1 || it + u < NP) {
                         ptx::mbar_arrive(&empty[scu[u]]);
                         if constexpr (NCEN > 0) ptx::mbar_arrive(&cempty[sku[u]]);
-                        if (it + u >= NP - G) ptx::mbar_arrive(&empty[su[u]]);
+                        if (ZH > 0 && it + u >= NP - ZH) ptx::mbar_arrive(&empty[su[u]]);
                     }
             }
 #pragma unroll
