@@ -347,27 +347,30 @@ class BatchedRK4Integrator {
         using Entry = treesap_b200::StageEntry<Cfg, R, Epi>;
         DevArray<Entry> entries;
         static auto kernel() { return &treesap_b200::batch_stage_kernel<Cfg, R, Epi>; }
-        static int grid(int sms) {
-            static int occ[64] = {0};
+        /// Persistent grid for tiles of `ty` rows: the CTAs of 32 ty + 32 threads that fit an SM
+        /// at once (registers and the ring's shared memory), times the SMs.
+        static int grid(int sms, int ty) {
+            static int occ[64][Cfg::TYMAX + 1] = {};
             int dev = 0;
             treesap_b200::cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
             if (dev < 0 || dev >= 64) dev = 0;
-            if (occ[dev] == 0) {
+            if (ty < 1 || ty > Cfg::TYMAX) ty = Cfg::TYMAX;
+            if (occ[dev][ty] == 0) {
                 using RingT = treesap_b200::Ring<Cfg, Epi>;
                 treesap_b200::cuda_check(
                     cudaFuncSetAttribute(kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, RingT::SMEM),
                     "cudaFuncSetAttribute(smem)");
                 int nb = 0;
                 treesap_b200::cuda_check(
-                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel(), Cfg::THREADS, RingT::SMEM),
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel(), 32 * ty + 32, RingT::SMEM),
                     "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-                occ[dev] = nb > 0 ? nb : 1;
+                occ[dev][ty] = nb > 0 ? nb : 1;
             }
-            return occ[dev] * sms;
+            return occ[dev][ty] * sms;
         }
         void launch(const DevArray<treesap_b200::ItemBox>& items, int ty, int* err, int sms, cudaStream_t s) const {
             using RingT = treesap_b200::Ring<Cfg, Epi>;
-            int g = grid(sms);
+            int g = grid(sms, ty);
             if (g > items.n) g = items.n;
             if (g < 1) return;
             // through the registered entry point, like StageLauncher::launch
