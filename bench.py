@@ -344,7 +344,7 @@ def run_b200(args, rank, world, local_rank):
     except Exception as ex:  # noqa: BLE001 - reported in the line
         batched = {"value": None, "error": str(ex)}
 
-    # tensor model (C3): a few steps of each form (the 12-component kernels are slow)
+    # tensor model (C3): a few steps of each form (the 12-component kernels take tens of ms per step)
     tensor = None
     try:
         from treesap_b200.run_tensor import run as run_tensor
