@@ -17,7 +17,9 @@ from scipy.special import erf
 from treesap_b200 import TSError, expression_eval
 
 ROOT = Path(__file__).resolve().parents[1]
-REF = Path("/root/reference")
+from conftest import REFERENCE_SKIP, reference_root  # noqa: E402
+
+REF = reference_root()
 
 rng = np.random.default_rng(123)
 X, Y, Z = rng.uniform(-1.0, 1.0, (3, 200))
@@ -62,7 +64,7 @@ def test_invalid_expressions_are_refused(text):
     assert e.value.status == 1
 
 
-@pytest.mark.skipif(not (REF / "examples").exists(), reason="reference sources not present")
+@pytest.mark.skipif(REF is None, reason=REFERENCE_SKIP)
 @pytest.mark.parametrize("example", ["examples/01-wave-eqn/main.cpp", "examples/02-temporaries/main.cpp"])
 def test_reference_example_driver_compiles_unchanged(tmp_path, example):
     """The reference's example programs (FunctionInit, PDEModel, RK4 integrator, exporter,

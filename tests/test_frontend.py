@@ -19,7 +19,9 @@ import pytest
 ROOT = Path(__file__).resolve().parents[1]
 INC = ["-I", str(ROOT / "include"), "-I", str(ROOT / "treesap_b200/cpp/compat"), "-I",
        str(ROOT / "treesap_b200/cpp/treesap"), "-I", str(ROOT / "treesap_b200/cpp/rhs")]
-REF = Path("/root/reference")
+from conftest import REFERENCE_SKIP, reference_root  # noqa: E402
+
+REF = reference_root()
 
 
 def first_w(n, p):
@@ -103,10 +105,24 @@ template class treesap::SingleLevelEulerIntegrator<Model>;
 '''
 
 
-@pytest.mark.skipif(not (REF / "examples").exists(), reason="reference sources not present")
+@pytest.mark.skipif(REF is None, reason=REFERENCE_SKIP)
 @pytest.mark.parametrize("header,rhs", [("examples/01-wave-eqn/WaveEqnRHS.hpp", "WaveEqnRHS<2>"),
                                         ("examples/02-temporaries/NonLinearRHS.hpp", "NonLinearRHS<1>")])
 def test_reference_example_rhs_compiles_unchanged(tmp_path, header, rhs):
     src = tmp_path / "dropin.cu"
     src.write_text(DROPIN % (str(REF / header), rhs))
     nvcc_compile(src, tmp_path / "dropin.o")
+
+
+def test_bounds_checked_view_flags_out_of_range_reads(tmp_path):
+    """TREESAP_B200_CHECK builds: the stencil view's range checks, run on the host (no GPU). An
+    out-of-range read sets bit 2 (index out of bounds) of the error word and reads the centre;
+    in-range reads are untouched. The GPU side of the same build is exercised by the
+    bounds-checked tile variants (tests/test_gpu_tile_variants.py)."""
+    exe = tmp_path / "check_view"
+    subprocess.run(["g++", "-std=c++20", "-O1", *INC, str(ROOT / "tests/cpp/check_view_probe.cpp"), "-o", str(exe)],
+                   check=True)
+    r = json.loads(subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout)
+    assert r["in_plane"] == 34 and r["in_glob"] == 1000 + (8 * 35 + 4 * 5 + 3) and r["err_in"] == 0
+    assert r["err_plane"] == 2 and r["out_plane"] == 17
+    assert r["err_glob"] == 2 and r["out_glob"] == 1000 + 4 * 35 + 17
