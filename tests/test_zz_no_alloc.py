@@ -51,15 +51,19 @@ def relerr(a, b):
     return float(np.abs(a - b).max() / np.abs(b).max())
 
 
-def test_noalloc_matches_allocating_path_on_two_calls(ctx):
-    import torch
-
-    desc = wave_desc((40, 36, 44), 2, periodic=(1, 0, 1), ko=0.1, bc=tsb.TS_BC_DIRICHLET, bc_values=(0.2, 0.0),
-                     dt=0.2 / 44)
-    rng = np.random.default_rng(7)
+def initial_state(rng):
     z, y, x = np.meshgrid(*(np.arange(m) / m for m in (44, 36, 40)), indexing="ij")
     s0 = np.stack([np.sin(2 * np.pi * (x + 2 * z)) * np.exp(-((y - 0.5) / 0.2) ** 2), 0.1 * np.cos(2 * np.pi * y)])
-    s0 += 0.01 * rng.standard_normal(s0.shape)
+    return s0 + 0.01 * rng.standard_normal(s0.shape)
+
+
+@pytest.mark.parametrize("bc", [tsb.TS_BC_DIRICHLET, tsb.TS_BC_NOOP])
+@pytest.mark.parametrize("ko", [0.0, 0.1])
+def test_noalloc_matches_allocating_path_on_two_calls(ctx, bc, ko):
+    import torch
+
+    desc = wave_desc((40, 36, 44), 2, periodic=(1, 0, 1), ko=ko, bc=bc, bc_values=(0.2, 0.0), dt=0.2 / 44)
+    s0 = initial_state(np.random.default_rng(7))
 
     ref = tsb.Integrator(ctx, desc)
     ref.set_state(s0)
@@ -68,6 +72,7 @@ def test_noalloc_matches_allocating_path_on_two_calls(ctx):
     ref.step(4)
     ref7 = ref.get_state()
     ctx.sync()
+    ref.close()
 
     L = layout_of(desc)
     dev = torch.from_numpy(to_padded(s0, L)).cuda()
@@ -79,6 +84,36 @@ def test_noalloc_matches_allocating_path_on_two_calls(ctx):
     assert f(C.byref(desc), dev.data_ptr(), 4, stream) == 0
     got7 = from_padded(dev.cpu().numpy(), L)
     assert relerr(got7, ref7) <= TOL
+
+
+def test_noalloc_zero_steps_leaves_the_state_unchanged():
+    import torch
+
+    desc = wave_desc((40, 36, 44), 2, periodic=(1, 0, 1), ko=0.1, bc=tsb.TS_BC_DIRICHLET, dt=0.2 / 44)
+    L = layout_of(desc)
+    pad = to_padded(initial_state(np.random.default_rng(11)), L)
+    dev = torch.from_numpy(pad).cuda()
+    assert noalloc_fn()(C.byref(desc), dev.data_ptr(), 0, None) == 0
+    assert np.array_equal(dev.cpu().numpy(), pad)
+
+
+def test_noalloc_allocates_no_device_memory():
+    """After a first call (which looks up the scratch array's address), further calls leave the
+    device's free memory unchanged: the stage registers come from the static array."""
+    import torch
+
+    desc = wave_desc((40, 36, 44), 2, periodic=(1, 0, 1), ko=0.1, bc=tsb.TS_BC_DIRICHLET, dt=0.2 / 44)
+    L = layout_of(desc)
+    dev = torch.from_numpy(to_padded(initial_state(np.random.default_rng(5)), L)).cuda()
+    f = noalloc_fn()
+    assert f(C.byref(desc), dev.data_ptr(), 1, None) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        assert f(C.byref(desc), dev.data_ptr(), 2, None) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
 
 
 def test_noalloc_refuses_domains_beyond_its_scratch():

@@ -162,16 +162,21 @@ extern "C" ts_status ts_wave_rk4_steps_noalloc(const ts_wave_desc* desc, double*
     unsigned char* base = nullptr;
     ts_status st = scratch_address(dev, &base);
     if (st != TS_OK) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // On an error part-way through, kernels already queued may still write to `state` and to
+    // the scratch array: wait for the stream (ignoring its status) before returning, so that
+    // no work of this call is in flight once it has returned.
     try {
-        cudaStream_t s = static_cast<cudaStream_t>(stream);
         if (d.ko_strength > 0.0)
             dispatch_bc(d, treesap::KODecorator<tsb::WaveRHS<2>>{tsb::WaveRHS<2>{}, d.ko_strength}, state, base, nsteps,
                         s);
         else
             dispatch_bc(d, tsb::WaveRHS<2>{}, state, base, nsteps, s);
     } catch (const std::domain_error&) {
+        (void)cudaStreamSynchronize(s);
         return TS_ERR_DEVICE;
     } catch (const std::exception&) {
+        (void)cudaStreamSynchronize(s);
         return TS_ERR_CUDA;
     }
     return TS_OK;
