@@ -22,16 +22,13 @@
 namespace tsb {
 
 namespace detail {
-/// sum_a KO_a of component n (the KODecorator's order of summation).
+/// base + s sum_a KO_a of component n, the KODecorator's arithmetic (its one-pass form), or
+/// base when s = 0.
 template <int G, typename T>
-AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE T ko_sum(const amrex::Array4<const T>& arr, int n, const amrex::IntVect& idx,
-                                                  const amrex::GeometryData& geom) {
-    using namespace treesap::stencil;
-    T ko = T(0);
-    ko += kreiss_oliger<G, dir::x>(arr, n, idx, geom);
-    ko += kreiss_oliger<G, dir::y>(arr, n, idx, geom);
-    ko += kreiss_oliger<G, dir::z>(arr, n, idx, geom);
-    return ko;
+AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE T with_ko(T base, const amrex::Array4<const T>& arr, int n,
+                                                   const amrex::IntVect& idx, const amrex::GeometryData& geom,
+                                                   amrex::Real s) {
+    return s > 0.0 ? treesap::stencil::kreiss_oliger_added<G>(base, arr, n, idx, geom, s) : base;
 }
 
 /// sum_a D2_aa of component n (WaveRHS's contraction order).
@@ -82,13 +79,12 @@ template <int ngrow_> struct WaveC2RHS {
         if constexpr (comp == 2) {
             return T(0);
         } else {
-            const T ko = ko_strength > 0.0 ? detail::ko_sum<ngrow>(arr, comp, idx, geom) : T(0);
             T base;
             if constexpr (comp == 0)
                 base = arr(idx, 1);
             else
                 base = arr(idx, 2) * detail::lap<ngrow>(arr, 0, idx, geom);
-            return ko_strength > 0.0 ? base + T(ko_strength) * ko : base;
+            return detail::with_ko<ngrow>(base, arr, comp, idx, geom, ko_strength);
         }
     }
 };
@@ -108,13 +104,12 @@ template <int ngrow_> struct WaveC2AdjointRHS {
         if constexpr (comp == 2) {
             return T(0);
         } else {
-            const T ko = ko_strength > 0.0 ? detail::ko_sum<ngrow>(arr, comp, idx, geom) : T(0);
             T base;
             if constexpr (comp == 0)
                 base = detail::lap_of_product<ngrow>(arr, 2, 1, idx, geom);
             else
                 base = arr(idx, 0);
-            return ko_strength > 0.0 ? base + T(ko_strength) * ko : base;
+            return detail::with_ko<ngrow>(base, arr, comp, idx, geom, ko_strength);
         }
     }
 };
@@ -154,7 +149,6 @@ template <int ngrow_> struct WaveAdjointSpeedRHS {
     AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE T operator()(const amrex::IntVect idx, amrex::Real,
                                                           const amrex::Array4<const T>& arr,
                                                           const amrex::GeometryData& geom, Workspace&) const {
-        const T ko = ko_strength > 0.0 ? detail::ko_sum<ngrow>(arr, comp, idx, geom) : T(0);
         T base;
         if constexpr (comp == 0) {
             using namespace treesap::stencil_impl;
@@ -180,7 +174,7 @@ template <int ngrow_> struct WaveAdjointSpeedRHS {
         } else {
             base = arr(idx, 0);
         }
-        return ko_strength > 0.0 ? base + T(ko_strength) * ko : base;
+        return detail::with_ko<ngrow>(base, arr, comp, idx, geom, ko_strength);
     }
 };
 
@@ -198,7 +192,6 @@ template <int ngrow_> struct WaveC2TangentRHS {
         if constexpr (comp == 2 || comp == 5) {
             return T(0);
         } else {
-            const T ko = ko_strength > 0.0 ? detail::ko_sum<ngrow>(arr, comp, idx, geom) : T(0);
             T base;
             if constexpr (comp == 0)
                 base = arr(idx, 1);
@@ -209,7 +202,7 @@ template <int ngrow_> struct WaveC2TangentRHS {
             else
                 base = arr(idx, 2) * detail::lap<ngrow>(arr, 3, idx, geom) +
                        arr(idx, 5) * detail::lap<ngrow>(arr, 0, idx, geom);
-            return ko_strength > 0.0 ? base + T(ko_strength) * ko : base;
+            return detail::with_ko<ngrow>(base, arr, comp, idx, geom, ko_strength);
         }
     }
 };

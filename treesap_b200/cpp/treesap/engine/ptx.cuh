@@ -17,6 +17,18 @@ enum DeviceError : int {
 };
 
 constexpr unsigned long long kWaitLimitNs = 2000000000ull; // 2 s
+/// Wait bound of a launch that carries an injected fault (ts_context_inject_fault).
+constexpr unsigned long long kInjectedWaitLimitNs = 1000000ull; // 1 ms
+
+/// Records `bit` in a device error word (atomically on the device; plain OR on the host).
+__host__ __device__ __forceinline__ void flag_error(int* err, int bit) {
+    if (!err) return;
+#if defined(__CUDA_ARCH__)
+    atomicOr(err, bit);
+#else
+    *err |= bit;
+#endif
+}
 
 namespace ptx {
 
@@ -49,6 +61,16 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+/// Arrives on `bar` when `pred` holds (predicated, no branch): the elected lane of a warp
+/// releasing a ring slot after __syncwarp().
+__device__ __forceinline__ void mbar_arrive_if(uint64_t* bar, bool pred) {
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %1, 0;\n\t"
+                 "@p mbarrier.arrive.shared::cta.b64 _, [%0];\n\t}" ::"r"(smem_addr(bar)),
+                 "r"(int(pred))
+                 : "memory");
 }
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {

@@ -42,6 +42,7 @@
 
 #include <cmath>
 #include <cuda_runtime.h>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -103,12 +104,17 @@ struct TileCfg {
 /// Shared-memory rings of one (tile configuration, epilogue) pair:
 ///   * the stencil ring, R = G + U + P slots, each one stencil plane ([comp][y][x], TY CY + 2G
 ///     rows of BX), with a `full` and an `empty` mbarrier per slot;
-///   * the centre-operand ring, RC = U + P slots (none without centre operands), each the
-///     epilogue's centre-operand boxes of one centre plane ([comp][y][x], TY CY rows of TX per
-///     field, 128-byte aligned), with an `empty` mbarrier per slot. The boxes of centre plane
-///     c are copied together with (and complete on the `full` barrier of) stencil plane c + G,
-///     the newest plane of the iteration that computes centre plane c.
-/// P is the configuration's prefetch depth, reduced until both rings fit the budget.
+///   * the centre-operand ring, RC slots (none without centre operands), each the epilogue's
+///     centre-operand boxes of one centre plane ([comp][y][x], TY CY rows of TX per field,
+///     128-byte aligned), with an `empty` mbarrier per slot. The boxes of centre plane c are
+///     copied together with (and complete on the `full` barrier of) stencil plane c + G, the
+///     newest plane of the iteration that computes centre plane c.
+/// Static layout (circular register queue, one plane per iteration): R equals the queue depth
+/// QL = 2G + 1 (P = G), so that in the plane loop, which is unrolled QL times, every stencil
+/// slot is a compile-time constant (single-item launches) and no slot counter is carried from
+/// plane to plane; the same holds for the centre ring when its size divides QL. Otherwise P is
+/// the configuration's prefetch depth, reduced until both rings fit the budget. The centre ring
+/// has up to U + P slots (as many as fit); fewer cap the prefetch depth at RC - 1 planes.
 template <class Cfg, class Epi> struct Ring {
     using C0 = typename Epi::C0;
     using C1 = typename Epi::C1;
@@ -118,18 +124,31 @@ template <class Cfg, class Epi> struct Ring {
     static constexpr int C0_OFF = 0; // within a centre slot
     static constexpr int C1_OFF = NCEN > 0 ? align128(Cfg::CBOX * int(sizeof(C0))) : 0;
     static constexpr int CSLOT = NCEN > 1 ? C1_OFF + align128(Cfg::CBOX * int(sizeof(C1))) : C1_OFF;
-    static constexpr int P = [] {
+    static constexpr int QL = 2 * Cfg::ZH + Cfg::U;
+    static constexpr int bytes(int r, int rc) { return r * (SSLOT + 16) + rc * (CSLOT + 8); }
+    /// Static layout: circular queue, one plane per iteration, and R = QL stencil slots fit.
+    static constexpr bool kStatic = Cfg::ROT && Cfg::U == 1 && Cfg::ZQ && bytes(QL, NCEN > 0 ? 1 : 0) <= Cfg::SMEM_BUDGET;
+    static constexpr int P = kStatic ? QL - Cfg::ZH - Cfg::U : [] {
         int p = Cfg::P;
         while (p > 1 && Cfg::smem_for(p, CSLOT) > Cfg::SMEM_BUDGET) --p;
         return p;
     }();
     static constexpr int R = Cfg::ZH + Cfg::U + P;
-    static constexpr int RC = NCEN > 0 ? Cfg::U + P : 0;
+    /// Centre ring: QL slots in the static layout when they fit (compile-time slots), else up to
+    /// U + P slots, as many as fit beside the stencil ring.
+    static constexpr int RC = [] {
+        if (NCEN > 0 && kStatic && bytes(R, QL) <= Cfg::SMEM_BUDGET) return QL;
+        int rc = NCEN > 0 ? Cfg::U + P : 0;
+        while (rc > 1 && bytes(R, rc) > Cfg::SMEM_BUDGET) --rc;
+        return rc;
+    }();
+    /// Centre-ring slots are compile-time constants too when RC divides QL.
+    static constexpr bool kStaticCentre = kStatic && (RC == 0 || QL % RC == 0);
     static constexpr int CRING_OFF = R * SSLOT;             // centre ring
     static constexpr int BAR_OFF = CRING_OFF + RC * CSLOT;  // full[R], empty[R], cempty[RC]
     static constexpr int SMEM = BAR_OFF + 8 * (2 * R + RC);
-    static_assert(Cfg::smem_for(P, CSLOT) <= Cfg::SMEM_BUDGET,
-                  "shared-memory rings too large for this tile configuration");
+    static_assert(!kStatic || R == QL, "static ring layout");
+    static_assert(bytes(R, RC) <= Cfg::SMEM_BUDGET, "shared-memory rings too large for this tile configuration");
 };
 
 /// Launch-invariant stage inputs.
@@ -142,6 +161,8 @@ template <typename T> struct StageParams {
     int ty;                   // consumer warps (a tile is ty * CY rows high), <= TYMAX
     int zchunk;               // planes per z chunk
     int* err;                 // device error word
+    unsigned long long wait_ns = kWaitLimitNs; // bound of every mbarrier wait of the launch
+    int skip_plane = -1; // injected fault: the producer skips the copy of this plane of every item
 };
 
 /// TMA descriptors of the centre-operand fields (box TX x ty CY x 1 x NC) and the storage
@@ -242,6 +263,7 @@ struct ItemBox {
 /// blockIdx / ntiles), everything else in kernel-parameter space.
 template <class Cfg, class RHS, class Epi> struct SingleSource {
     using T = typename Cfg::T;
+    static constexpr bool kSingleItem = true; // at most one item per CTA: rings start at slot 0
     const CUtensorMap* tmap;
     const CentreMaps* cmaps;
     const StageParams<T>* sp;
@@ -281,6 +303,7 @@ template <class Cfg, class RHS, class Epi> struct alignas(64) StageEntry {
 /// of a host-built list (instances of any size, tiles x z ranges, longest first).
 template <class Cfg, class RHS, class Epi> struct BatchSource {
     using T = typename Cfg::T;
+    static constexpr bool kSingleItem = false;
     using Entry = StageEntry<Cfg, RHS, Epi>;
     const Entry* entries;
     const ItemBox* items;
@@ -351,8 +374,11 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
             RingPos ps, pc;
             long long t = 0, tc = 0;
             bool ok = true;
+            unsigned long long wl = kWaitLimitNs;
             for (int m = 0; m < nitems && ok; ++m) {
                 const ItemBox b = src.item(m);
+                const int skip = src.params(b.inst).skip_plane;
+                wl = src.params(b.inst).wait_ns;
                 const CUtensorMap* tmap = src.stencil_map(b.inst);
                 const CentreMaps& cm = src.centre_maps(b.inst);
                 ptx::prefetch_tensor_map(tmap);
@@ -367,14 +393,26 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
                 }
                 const int NP = (b.z1 - b.z0) + 2 * ZH; // planes z0 - ZH .. z1 - 1 + ZH
                 for (int q = 0; q < NP; ++q, ++t) {
-                    if (t >= R && !ptx::mbar_wait(&empty[ps.s], ps.ph ^ 1u, err)) {
+                    if (t >= R && !ptx::mbar_wait(&empty[ps.s], ps.ph ^ 1u, err, wl)) {
                         ok = false;
                         break;
                     }
                     const bool centre = NCEN > 0 && q >= 2 * ZH;
-                    if (centre && tc >= RC && !ptx::mbar_wait(&cempty[pc.s], pc.ph ^ 1u, err)) {
+                    if (centre && tc >= RC && !ptx::mbar_wait(&cempty[pc.s], pc.ph ^ 1u, err, wl)) {
                         ok = false;
                         break;
+                    }
+                    if (q == skip) {
+                        // injected fault: this plane's copy is never issued, so its `full`
+                        // barrier never completes and the consumers' bounded waits expire
+                        if constexpr (NCEN > 0) {
+                            if (centre) {
+                                pc.next(RC);
+                                ++tc;
+                            }
+                        }
+                        ps.next(R);
+                        continue;
                     }
                     ptx::mbar_arrive_expect_tx(&full[ps.s], bytes + (centre ? cbytes : 0u));
                     // storage coordinates: x = x0 - XH + xoff (= x0), y = y0 - G + g (= y0), z = z0 - G + q + g
@@ -397,8 +435,9 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
             }
             if (!ok) {
                 // a consumer warp stopped releasing slots: let the copies in flight land
+                // (bounded: a plane whose copy was never issued completes nothing)
                 for (long long r = (t > R ? t - R : 0); r < t; ++r)
-                    ptx::mbar_wait(&full[r % R], uint32_t((r / R) & 1), nullptr, 100000000ull);
+                    ptx::mbar_wait(&full[r % R], uint32_t((r / R) & 1), nullptr, wl < 100000000ull ? wl : 100000000ull);
             }
         }
         return;
@@ -408,6 +447,10 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
     // -------------------------------------------------------------------- consumer warps
     constexpr int CX = Cfg::CX, U = Cfg::U;
     constexpr int QL = 2 * ZH + U; // register queue depth (planes)
+    // compile-time ring slots: static layout and one item per CTA (the rings start at slot 0)
+    constexpr bool kStaticPos = RingT::kStatic && Src::kSingleItem;
+    constexpr bool kStaticCen = RingT::kStaticCentre && Src::kSingleItem;
+    const bool leader = lane == 0; // the lane that releases ring slots for its warp
     constexpr int NCOL = CY * CX;  // columns (cells per plane) of a thread: column r CX + e is cell (i0 + e, j0 + r)
     const int tx = lane, ty = warp;
     const int coff = (CY * ty + G) * BX + (CX * tx + XH); // cell (i0, j0)'s centre inside the stencil plane (row r: + r BX)
@@ -427,6 +470,7 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
         const Layout L = spr.L;
         const double time = spr.time;
         const T* const in = spr.in;
+        const unsigned long long wl = spr.wait_ns;
         const typename Epi::Params epl = src.epi(b.inst);
 
         const int NP = (b.z1 - b.z0) + 2 * ZH;
@@ -455,9 +499,12 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
 #pragma unroll
         for (int p = 0; p < 2 * ZH; ++p) {
             if (p == ZH) cpos = pos;
-            if (ok && !ptx::mbar_wait(&full[pos.s], pos.ph, err)) ok = false;
+            // static layout: plane p of the only item sits in slot p (p < 2G < R), first phase
+            const int ps = kStaticPos ? p : pos.s;
+            const uint32_t pph = kStaticPos ? 0u : pos.ph;
+            if (ok && !ptx::mbar_wait(&full[ps], pph, err, wl)) ok = false;
             if (ok) {
-                const T* pl = reinterpret_cast<const T*>(smem_raw + pos.s * SSLOT) + coff;
+                const T* pl = reinterpret_cast<const T*>(smem_raw + ps * SSLOT) + coff;
 #pragma unroll
                 for (int r = 0; r < CY; ++r)
 #pragma unroll
@@ -469,10 +516,10 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
                     }
                 if (p < ZH || p >= NP - ZH) {
                     __syncwarp();
-                    if (lane == 0) ptx::mbar_arrive(&empty[pos.s]);
+                    ptx::mbar_arrive_if(&empty[ps], leader);
                 }
             }
-            pos.next(R);
+            if constexpr (!kStaticPos) pos.next(R);
         }
         if (!ok) break;
 
@@ -481,20 +528,29 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
         // Circular queue (ROT): plane p lives in slot p % QL, the loop is unrolled QL times and
         // unrolled copy k (it = 2G + k mod QL) finds offset dk of its centre in slot (G + dk + k) % QL.
         constexpr int KU = Cfg::ROT ? QL : 1;
-        for (int base = 2 * ZH; base < NP && ok; base += KU * U)
+        uint32_t mph = 0; // static layout: parity of the QL-plane block of this base iteration
+        for (int base = 2 * ZH; base < NP && ok; base += KU * U, mph ^= 1u)
 #pragma unroll
         for (int k = 0; k < KU; ++k) {
             const int it = base + k * U;
             if (Cfg::ROT && it >= NP) break;
             int su[U], scu[U], sku[U];
-            {
+            if constexpr (kStaticPos) {
+                // it = 2G + QL m + k with R = QL: newest plane in slot (2G + k) % R, in its
+                // (m + (2G + k) / R)-th use; centre plane it - G in slot (G + k) % R; centre
+                // operands (it - 2G = QL m + k) in slot k % RC when RC divides QL
+                su[0] = (2 * ZH + k) % R;
+                scu[0] = (ZH + k) % R;
+                sku[0] = NCEN == 0 ? 0 : (kStaticCen ? k % RC : kpos.s);
+                if (!ptx::mbar_wait(&full[su[0]], mph ^ uint32_t(((2 * ZH + k) / R) & 1), err, wl)) ok = false;
+            } else {
                 RingPos pp = pos, cp = cpos, kp = kpos;
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     su[u] = pp.s;
                     scu[u] = cp.s;
                     sku[u] = kp.s;
-                    if (it + u < NP && !ptx::mbar_wait(&full[pp.s], pp.ph, err)) ok = false;
+                    if (it + u < NP && !ptx::mbar_wait(&full[pp.s], pp.ph, err, wl)) ok = false;
                     pp.next(R);
                     cp.next(R);
                     if constexpr (NCEN > 0) kp.next(RC);
@@ -573,6 +629,19 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
                                                         CX == 2 ? &xwin[0][0] : nullptr,
                                                         XWN,
                                                         GW + e};
+#ifdef TREESAP_B200_CHECK
+#pragma unroll
+                    for (int e = 0; e < CX; ++e) {
+                        // bounds of the stencil slot and of the input field around this cell
+                        const int pofs = coff + r * BX + e;
+                        const long long gofs = L.index(i0 + e, j0 + r, z, 0);
+                        view[e].err = err;
+                        view[e].plo = -pofs;
+                        view[e].phi = NC * PNS - pofs;
+                        view[e].glo = -gofs;
+                        view[e].ghi = L.elements() - gofs;
+                    }
+#endif
                     bool whole = U == 1 || it + u < NP;
 #pragma unroll
                     for (int e = 0; e < CX; ++e) whole = whole && act[r][e];
@@ -612,22 +681,24 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
                 }
             }
             __syncwarp();
-            if (lane == 0) {
 #pragma unroll
-                for (int u = 0; u < U; ++u)
-                    if (U == 1 || it + u < NP) {
-                        ptx::mbar_arrive(&empty[scu[u]]);
-                        if constexpr (NCEN > 0) ptx::mbar_arrive(&cempty[sku[u]]);
-                        if (ZH > 0 && it + u >= NP - ZH) ptx::mbar_arrive(&empty[su[u]]);
-                    }
-            }
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
+            for (int u = 0; u < U; ++u)
                 if (U == 1 || it + u < NP) {
-                    pos.next(R);
-                    cpos.next(R);
-                    if constexpr (NCEN > 0) kpos.next(RC);
+                    ptx::mbar_arrive_if(&empty[scu[u]], leader);
+                    if constexpr (NCEN > 0) ptx::mbar_arrive_if(&cempty[sku[u]], leader);
+                    if (ZH > 0 && it + u >= NP - ZH) ptx::mbar_arrive_if(&empty[su[u]], leader);
                 }
+            if constexpr (!kStaticPos) {
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    if (U == 1 || it + u < NP) {
+                        pos.next(R);
+                        cpos.next(R);
+                        if constexpr (NCEN > 0) kpos.next(RC);
+                    }
+                }
+            } else if constexpr (NCEN > 0 && !kStaticCen) {
+                kpos.next(RC);
             }
         }
     }
@@ -881,14 +952,43 @@ template <class Cfg> LaunchShape make_shape(const Layout& L, int slots, int ty, 
     return s;
 }
 
+/// Resident CTAs per SM of the kernel `K` launched with 32 ty + 32 threads and `smem` bytes of
+/// dynamic shared memory, cached per device and tile height; the kernel's dynamic shared-memory
+/// limit is raised on the device's first query. A lock guards the cache: integrators on several
+/// host threads may query it at once.
+template <auto K, int TYMAX> int cached_occupancy(int ty, int smem) {
+    static std::mutex m;
+    static int occ[64][TYMAX + 1] = {};
+    static bool attr[64] = {};
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= 64) throw std::runtime_error("device ordinal beyond the occupancy cache");
+    if (ty < 1 || ty > TYMAX) ty = TYMAX;
+    std::lock_guard<std::mutex> lock(m);
+    if (!attr[dev]) {
+        cuda_check(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                   "cudaFuncSetAttribute(smem)");
+        attr[dev] = true;
+    }
+    if (occ[dev][ty] == 0) {
+        int nb = 0;
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, K, 32 * ty + 32, smem),
+                   "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        occ[dev][ty] = nb > 0 ? nb : 1;
+    }
+    return occ[dev][ty];
+}
+
 /// Tile height for a given width in x: the largest ty <= TYMAX whose tile count fills the SMs
 /// most evenly (fraction of busy slot-time in the last wave), ties to the taller tile.
-template <class Cfg> int choose_ty(const Layout& L, int slots) {
+/// `slots(ty)`: resident CTA slots of the whole GPU for tiles of ty rows.
+template <class Cfg, class SlotsFn> int choose_ty(const Layout& L, SlotsFn&& slots) {
     int best = Cfg::TYMAX;
     double best_eff = -1.0;
     for (int ty = Cfg::TYMAX; ty >= (Cfg::TYMAX + 1) / 2; --ty) {
-        const LaunchShape s = make_shape<Cfg>(L, slots, ty);
-        const double waves = double(s.grid) / slots;
+        const int sl = slots(ty);
+        const LaunchShape s = make_shape<Cfg>(L, sl, ty);
+        const double waves = double(s.grid) / sl;
         const double eff = waves / std::ceil(waves) * (double(ty) / Cfg::TYMAX > 0.75 ? 1.0 : 0.95);
         if (eff > best_eff + 1e-9) {
             best_eff = eff;
@@ -901,27 +1001,13 @@ template <class Cfg> int choose_ty(const Layout& L, int slots) {
 template <class Cfg, class RHS, class Epi> struct StageLauncher {
     using RingT = Ring<Cfg, Epi>;
     static auto kernel() { return &stage_kernel<Cfg, RHS, Epi>; }
-    /// Resident CTAs per SM for this instantiation (sets the dynamic shared-memory limit once per device).
-    static int occupancy() {
-        static int occ[64] = {0};
-        int dev = 0;
-        cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
-        if (dev < 0 || dev >= 64) dev = 0;
-        if (occ[dev] == 0) {
-            cuda_check(cudaFuncSetAttribute(kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, RingT::SMEM),
-                       "cudaFuncSetAttribute(smem)");
-            int nb = 0;
-            cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel(), Cfg::THREADS, RingT::SMEM),
-                       "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-            occ[dev] = nb > 0 ? nb : 1;
-        }
-        return occ[dev];
-    }
+    /// Resident CTAs per SM for tiles of `ty` rows.
+    static int occupancy(int ty) { return cached_occupancy<&stage_kernel<Cfg, RHS, Epi>, Cfg::TYMAX>(ty, RingT::SMEM); }
     /// Launch shape for a layout; `ty` <= 0 picks the tile height, `nchunks` <= 0 the z split.
+    /// The z split fills the resident CTA slots of the chosen tile height.
     static LaunchShape shape(const Layout& L, int sm_count, int ty = 0, int nchunks = 0) {
-        const int slots = occupancy() * sm_count;
-        if (ty <= 0 || ty > Cfg::TYMAX) ty = choose_ty<Cfg>(L, slots);
-        return make_shape<Cfg>(L, slots, ty, nchunks);
+        if (ty <= 0 || ty > Cfg::TYMAX) ty = choose_ty<Cfg>(L, [&](int t) { return occupancy(t) * sm_count; });
+        return make_shape<Cfg>(L, occupancy(ty) * sm_count, ty, nchunks);
     }
     /// The TMA box of the stencil input for a launch shape: (TX + 2 XH) x (ty CY + 2G).
     static int box_x() { return Cfg::BX; }

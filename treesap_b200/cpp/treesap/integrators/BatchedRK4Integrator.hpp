@@ -350,23 +350,10 @@ class BatchedRK4Integrator {
         /// Persistent grid for tiles of `ty` rows: the CTAs of 32 ty + 32 threads that fit an SM
         /// at once (registers and the ring's shared memory), times the SMs.
         static int grid(int sms, int ty) {
-            static int occ[64][Cfg::TYMAX + 1] = {};
-            int dev = 0;
-            treesap_b200::cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
-            if (dev < 0 || dev >= 64) dev = 0;
-            if (ty < 1 || ty > Cfg::TYMAX) ty = Cfg::TYMAX;
-            if (occ[dev][ty] == 0) {
-                using RingT = treesap_b200::Ring<Cfg, Epi>;
-                treesap_b200::cuda_check(
-                    cudaFuncSetAttribute(kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, RingT::SMEM),
-                    "cudaFuncSetAttribute(smem)");
-                int nb = 0;
-                treesap_b200::cuda_check(
-                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel(), 32 * ty + 32, RingT::SMEM),
-                    "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-                occ[dev][ty] = nb > 0 ? nb : 1;
-            }
-            return occ[dev][ty] * sms;
+            using RingT = treesap_b200::Ring<Cfg, Epi>;
+            return treesap_b200::cached_occupancy<&treesap_b200::batch_stage_kernel<Cfg, R, Epi>, Cfg::TYMAX>(
+                       ty, RingT::SMEM) *
+                   sms;
         }
         void launch(const DevArray<treesap_b200::ItemBox>& items, int ty, int* err, int sms, cudaStream_t s) const {
             using RingT = treesap_b200::Ring<Cfg, Epi>;
@@ -485,6 +472,7 @@ class BatchedRK4Integrator {
                 e.cmaps.y[k] = c.L.g;
                 e.cmaps.z[k] = c.L.g;
             }
+            e.sp = treesap_b200::StageParams<typename Cfg::T>{}; // the entry's storage is raw memory
             e.sp.in = static_cast<const typename Cfg::T*>(input);
             e.sp.L = L;
             e.sp.geom = in.geom;

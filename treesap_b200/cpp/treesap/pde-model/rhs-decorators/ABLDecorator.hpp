@@ -62,8 +62,11 @@ struct ABLDecorator {
             ws.sigma_value = sigma_in<T>(idx);
             ws.have_sigma = true;
         }
-        return T(rhs.template operator()<comp>(idx, time, arr, geom, ws.inner)) -
-               T(ws.sigma_value) * (arr(idx, comp) - T(data.target_values[comp]));
+        const T inner = T(rhs.template operator()<comp>(idx, time, arr, geom, ws.inner));
+        // Inside the bulk sigma is 0 and the damping term vanishes: skip it (for finite states
+        // F - 0 (u - target) is F; whole warps of bulk cells take this branch together).
+        if (ws.sigma_value == 0.0) return inner;
+        return inner - T(ws.sigma_value) * (arr(idx, comp) - T(data.target_values[comp]));
     }
 
     /// 0 inside the bulk (where the clamped distance vanishes), else the profile of the

@@ -1,5 +1,7 @@
 // treesap-b200: Kreiss-Oliger dissipation decorator (reference pde-model/rhs-decorators/KODecorator.hpp:32-74).
 //   F -> F + strength * (D_KO^x + D_KO^y + D_KO^z) arr(., comp),   order defaults to ngrow.
+// The three directions are summed in one reassociated pass (stencil::kreiss_oliger_added),
+// which differs from the reference's direction-by-direction sum only by rounding.
 // Aggregate {rhs, strength} like the reference. The operator is templated on the value type
 // of the array so the same decorator runs in the FP32 stage form.
 #pragma once
@@ -25,12 +27,9 @@ struct KODecorator {
     AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE T operator()(const amrex::IntVect idx, amrex::Real time,
                                                           const amrex::Array4<const T>& arr,
                                                           const amrex::GeometryData& geom, Workspace& ws) const {
-        using namespace stencil;
-        T ko_term = T(0);
-        ko_term += kreiss_oliger<order, dir::x>(arr, comp, idx, geom);
-        ko_term += kreiss_oliger<order, dir::y>(arr, comp, idx, geom);
-        ko_term += kreiss_oliger<order, dir::z>(arr, comp, idx, geom);
-        return T(rhs.template operator()<comp>(idx, time, arr, geom, ws)) + T(strength) * ko_term;
+        // F + strength (KO_x + KO_y + KO_z), all three directions in one reassociated pass
+        return stencil::kreiss_oliger_added<order>(T(rhs.template operator()<comp>(idx, time, arr, geom, ws)), arr,
+                                                   comp, idx, geom, strength);
     }
 
     /// The decorator is linear, so its linear part decorates the inner linear part.
