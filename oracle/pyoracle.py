@@ -131,3 +131,36 @@ def cpu_model() -> str:
 
 def host_cores() -> int:
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+EXAMPLES_REF_LIB = HERE / "_ref" / "libtsref_examples.so"
+EXAMPLES_GPU_LIB = HERE / "_ref" / "libtsb_examples.so"
+EXAMPLE_NCOMP = {1: 4, 2: 2, 3: 2}
+
+
+class ExampleRunner:
+    """The reference's example models (and the test-only DerivativeProbeRHS) on either side of
+    the example parity tests: `side="ref"` runs the reference integrators on the host
+    (libtsref_examples.so), `side="gpu"` the B200 front end (libtsb_examples.so). Both are
+    built by the oracle recipe from the same model sources (tests/cpp/examples_run.hpp)."""
+
+    def __init__(self, side: str):
+        path = EXAMPLES_REF_LIB if side == "ref" else EXAMPLES_GPU_LIB
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (make -C oracle with the reference sources present)")
+        self.lib = C.CDLL(str(path))
+        self.fn = getattr(self.lib, "tsref_example_run" if side == "ref" else "tsb_example_run")
+        self.fn.restype = C.c_int
+        self.fn.argtypes = [C.c_int, C.POINTER(RefDesc), C.c_double, C.c_void_p, C.c_int, C.c_void_p]
+
+    def run(self, example: int, desc: RefDesc, state: np.ndarray, nsteps: int, param: float = 0.0) -> np.ndarray:
+        st = np.ascontiguousarray(state, dtype=np.float64)
+        out = np.zeros_like(st)
+        rc = self.fn(example, C.byref(desc), param, st.ctypes.data, nsteps, out.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"example run returned {rc}")
+        return out
+
+
+def examples_available(side: str) -> bool:
+    return (EXAMPLES_REF_LIB if side == "ref" else EXAMPLES_GPU_LIB).exists()
