@@ -37,7 +37,8 @@ typedef enum ts_status {
     TS_ERR_CUDA = 3,             /* a CUDA runtime call failed (text in ts_context_last_error) */
     TS_ERR_OUT_OF_MEMORY = 4,
     TS_ERR_DEVICE = 5,           /* a kernel reported an error word (bounded wait expired, bad index) */
-    TS_ERR_NO_DEVICE = 6         /* no usable sm_100 device */
+    TS_ERR_NO_DEVICE = 6,        /* no usable sm_100 device */
+    TS_ERR_NONFINITE = 7         /* ts_integrator_check_finite found a NaN or infinite state value */
 } ts_status;
 
 typedef enum ts_dtype { TS_F64 = 0, TS_F32 = 1 } ts_dtype;
@@ -72,6 +73,24 @@ TS_API const char* ts_context_last_error(const ts_context* ctx);
 TS_API void* ts_context_stream(ts_context* ctx);
 TS_API int* ts_context_error_word(ts_context* ctx);
 TS_API int ts_context_sm_count(const ts_context* ctx);
+
+/* Failure injection (test and diagnostic hooks; no counterpart in the reference, which aborts
+ * inside AMReX on errors). Nothing here faults, traps or hangs a GPU:
+ *   TS_FAULT_SKIP_COPY: in the next fused stage launch of a single-box integrator on this
+ *     context, the producer warps skip the TMA copy of item plane `arg` (>= 0) and every
+ *     mbarrier wait of that launch gives up after 1 ms instead of 2 s. The consumer warps that
+ *     needed the plane time out, record kErrMbarTimeout in the device error word and return;
+ *     the next ts_context_sync reports TS_ERR_DEVICE and clears the word. One-shot.
+ *   TS_FAULT_ALLOC: the next `arg` device field allocations made on the calling host thread
+ *     fail as out of memory (no cudaMalloc is made), so the entry point that allocates returns
+ *     TS_ERR_OUT_OF_MEMORY. arg = 0 clears it.
+ *   TS_FAULT_NONE: clears both. */
+typedef enum ts_fault { TS_FAULT_NONE = 0, TS_FAULT_SKIP_COPY = 1, TS_FAULT_ALLOC = 2 } ts_fault;
+TS_API ts_status ts_context_inject_fault(ts_context* ctx, int fault, long long arg);
+/* Used by the header front end when it builds a stage launch: takes (and clears) the pending
+ * TS_FAULT_SKIP_COPY of the context. Returns 1 with *plane and *wait_ns set when one is
+ * pending, else 0. */
+TS_API int ts_context_take_stage_fault(ts_context* ctx, int* plane, unsigned long long* wait_ns);
 
 /* ------------------------------------------------------------------ field layout */
 typedef struct ts_field_layout {
@@ -170,6 +189,9 @@ TS_API ts_status ts_integrator_state_field(ts_integrator* it, void** device_ptr,
 /* Capture one step into a CUDA graph and replay it for subsequent ts_integrator_step calls
  * (enable != 0), or go back to per-kernel launches (enable == 0). */
 TS_API ts_status ts_integrator_use_graph(ts_integrator* it, int enable);
+/* Health check (no counterpart in the reference): waits for the integrator's stream and scans
+ * the valid cells of the state; TS_ERR_NONFINITE when any value is NaN or infinite. */
+TS_API ts_status ts_integrator_check_finite(ts_integrator* it);
 
 /* Device time of the most recent ts_integrator_step call, measured with CUDA events on the
  * context stream (valid after ts_context_sync), and the number of kernels it launched. */
@@ -254,7 +276,8 @@ TS_API ts_status ts_adjoint_tangent(ts_adjoint* a, const double* phi0, const dou
  * caller's other streams. Advances `state` (a caller-owned device buffer in the layout of
  * ts_field_layout_make(n, 2, 2, TS_F64), ghost cells included) by nsteps RK4 steps with the
  * same fused stage kernels and ghost fills as ts_integrator_step, on `stream` (a
- * cudaStream_t, 0 = the legacy default stream), and waits for it. Supported: TS_MODEL_WAVE,
+ * cudaStream_t, 0 = the legacy default stream), and waits for it, on errors as well: when
+ * the call returns, none of its GPU work is still in flight. Supported: TS_MODEL_WAVE,
  * ngrow 2, optional Kreiss-Oliger, periodic / Dirichlet / NoOp boundaries, TS_RK4 in FP64;
  * anything else returns TS_ERR_UNSUPPORTED. Simulation time restarts at 0 on every call (the
  * supported models do not depend on time).

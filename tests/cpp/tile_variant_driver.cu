@@ -61,7 +61,13 @@ int main(int argc, char** argv) {
         run<treesap::SingleLevelRK4Integrator<Model>>(all, 12);
         run<treesap::SingleLevelRK4F32StageIntegrator<Model>>(all, 12);
     }
+    // the device error word must be clear (checked builds record out-of-range indices there)
+    const ts_status st = ts_context_sync(treesap_b200::default_context());
     amrex::Finalize();
+    if (st != TS_OK) {
+        std::fprintf(stderr, "device error: %s\n", ts_context_last_error(treesap_b200::default_context()));
+        return 5;
+    }
     FILE* f = std::fopen(argv[1], "wb");
     if (!f) return 3;
     const bool ok = std::fwrite(all.data(), sizeof(double), all.size(), f) == all.size();

@@ -33,6 +33,9 @@ __all__ = [
     "TS_INIT_FOURIER",
     "TS_MODEL_WAVE",
     "TS_MODEL_TENSOR_WAVE",
+    "TS_FAULT_NONE",
+    "TS_FAULT_SKIP_COPY",
+    "TS_FAULT_ALLOC",
 ]
 
 LIB_PATH = Path(__file__).resolve().with_name("libtreesap_b200.so")
@@ -51,7 +54,9 @@ STATUS_NAMES = {
     4: "TS_ERR_OUT_OF_MEMORY",
     5: "TS_ERR_DEVICE",
     6: "TS_ERR_NO_DEVICE",
+    7: "TS_ERR_NONFINITE",
 }
+TS_FAULT_NONE, TS_FAULT_SKIP_COPY, TS_FAULT_ALLOC = 0, 1, 2
 
 
 class TSError(RuntimeError):
@@ -128,6 +133,8 @@ def lib() -> C.CDLL:
         "ts_context_stream": (vp, [vp]),
         "ts_context_error_word": (vp, [vp]),
         "ts_context_sm_count": (i, [vp]),
+        "ts_context_inject_fault": (i, [vp, i, ll]),
+        "ts_context_take_stage_fault": (i, [vp, C.POINTER(i), C.POINTER(C.c_ulonglong)]),
         "ts_field_layout_make": (i, [C.POINTER(i), i, i, i, C.POINTER(FieldLayout)]),
         "ts_field_bytes": (ll, [C.POINTER(FieldLayout)]),
         "ts_field_tensor_map": (i, [C.POINTER(FieldLayout), vp, i, i, vp]),
@@ -142,6 +149,7 @@ def lib() -> C.CDLL:
         "ts_integrator_time": (i, [vp, C.POINTER(d), C.POINTER(ll)]),
         "ts_integrator_state_field": (i, [vp, C.POINTER(vp), C.POINTER(FieldLayout)]),
         "ts_integrator_use_graph": (i, [vp, i]),
+        "ts_integrator_check_finite": (i, [vp]),
         "ts_integrator_last_step_timing": (i, [vp, C.POINTER(d), C.POINTER(ll)]),
         "ts_integrator_profile": (i, [vp, i, i, C.POINTER(ll), C.POINTER(d)]),
         "ts_integrator_set_launch_shape": (i, [vp, i, i]),
@@ -194,6 +202,10 @@ class Context:
 
     def sync(self) -> None:
         _check(lib().ts_context_sync(self.handle), "ts_context_sync", self)
+
+    def inject_fault(self, fault: int, arg: int = 0) -> None:
+        """Test hook (ts_context_inject_fault): TS_FAULT_SKIP_COPY / TS_FAULT_ALLOC / TS_FAULT_NONE."""
+        _check(lib().ts_context_inject_fault(self.handle, fault, arg), "ts_context_inject_fault", self)
 
     @property
     def stream(self) -> int:
@@ -270,6 +282,10 @@ class Integrator:
             "ts_integrator_run",
             self.ctx,
         )
+
+    def check_finite(self) -> None:
+        """Raises TSError(TS_ERR_NONFINITE) when the state holds NaN or infinite values."""
+        _check(lib().ts_integrator_check_finite(self.handle), "ts_integrator_check_finite", self.ctx)
 
     def use_graph(self, enable: bool = True) -> None:
         _check(lib().ts_integrator_use_graph(self.handle, int(enable)), "ts_integrator_use_graph", self.ctx)

@@ -154,17 +154,49 @@ template <class U> struct StencilView {
     int qlen = 0;
     const U* xw = nullptr; // registers: the centre row around the cell, [qnc][xwn], offset di at xw0 + di
     int xwn = 0, xw0 = 0;
+#ifdef TREESAP_B200_CHECK
+    // Checked builds: the valid index ranges of the shared-memory plane [plo, phi) and of the
+    // global field [glo, ghi), relative to `plane` and `glob`; an access outside them sets bit 2
+    // (index out of bounds) of the device error word `err` and reads the centre instead.
+    int* err = nullptr;
+    int plo = 0, phi = 0;
+    Long glo = 0, ghi = 0;
+    AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE void flag_bounds() const {
+        if (!err) return;
+#if defined(__CUDA_ARCH__)
+        atomicOr(err, 2);
+#else
+        *err |= 2;
+#endif
+    }
+#endif
 
     AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE const U& at(int i, int j, int k, int n) const {
         const int di = i - ci, dj = j - cj, dk = k - ck;
         if (xw != nullptr && dk == 0 && dj == 0 && xw0 + di >= 0 && xw0 + di < xwn && n < qnc)
             return xw[n * xwn + xw0 + di];
-        if (dk == 0) return plane[n * pns + dj * pjs + di];
+        if (dk == 0) {
+            const int o = n * pns + dj * pjs + di;
+#ifdef TREESAP_B200_CHECK
+            if (o < plo || o >= phi) {
+                flag_bounds();
+                return plane[0];
+            }
+#endif
+            return plane[o];
+        }
         if (di == 0 && dj == 0 && dk >= -qg && dk <= qg && n < qnc) {
             const int m = dk + qg + qrot;
             return queue[(qlen > 0 ? m % qlen : m) * qnc + n];
         }
-        return glob[n * gns + dk * gks + dj * gjs + di];
+        const Long o = n * gns + dk * gks + dj * gjs + di;
+#ifdef TREESAP_B200_CHECK
+        if (o < glo || o >= ghi) {
+            flag_bounds();
+            return glob[0];
+        }
+#endif
+        return glob[o];
     }
 };
 

@@ -157,6 +157,7 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
     }
 
     virtual ~SingleLevelIntegrator() {
+        if (finite_flag) cudaFree(finite_flag);
         if (staging) cudaFree(staging);
         if (bc_recs_dev) cudaFree(bc_recs_dev);
     }
@@ -225,6 +226,20 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
         if (!dst_on_device) treesap_b200::cuda_check(cudaStreamSynchronize(stream()), "cudaStreamSynchronize");
     }
 
+    /// Health check: waits for the stream and reports whether every valid cell of the state is
+    /// finite (no NaN, no infinity).
+    bool state_is_finite() {
+        if (!finite_flag)
+            treesap_b200::cuda_check(cudaMalloc(&finite_flag, sizeof(int)), "cudaMalloc(finite flag)");
+        treesap_b200::cuda_check(cudaMemsetAsync(finite_flag, 0, sizeof(int), stream()), "cudaMemsetAsync(flag)");
+        treesap_b200::launch_nonfinite(state_old.data(), state_old.layout(), finite_flag, sm_count(), stream());
+        int h = 0;
+        treesap_b200::cuda_check(cudaMemcpyAsync(&h, finite_flag, sizeof(int), cudaMemcpyDeviceToHost, stream()),
+                                 "cudaMemcpyAsync(flag)");
+        treesap_b200::cuda_check(cudaStreamSynchronize(stream()), "cudaStreamSynchronize");
+        return h == 0;
+    }
+
     /// Attach (or detach with nullptr) a per-launch device clock.
     void attach_clock(KernelClock* c) { clock_ = c; }
 
@@ -286,6 +301,17 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
         clock_end();
     }
 
+    /// Applies a pending injected stage fault of the context (ts_context_inject_fault,
+    /// TS_FAULT_SKIP_COPY) to the launch about to be enqueued.
+    template <class T> void take_stage_fault(treesap_b200::StageParams<T>& sp) {
+        int plane = -1;
+        unsigned long long wait_ns = 0;
+        if (ts_context_take_stage_fault(ctx, &plane, &wait_ns)) {
+            sp.skip_plane = plane;
+            sp.wait_ns = wait_ns;
+        }
+    }
+
     const CUtensorMap& tensor_map(const void* base, const treesap_b200::Layout& L, int dtype, int box_x, int box_y) {
         return tmaps.get(base, L, dtype, box_x, box_y);
     }
@@ -323,6 +349,7 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
     Field state_new;
     amrex::BCRec* bc_recs_dev = nullptr;
     double* staging = nullptr;
+    int* finite_flag = nullptr; // device flag of state_is_finite()
     treesap_b200::TensorMapCache tmaps;
     long long launches_per_step_ = 0;
     long long fills_this_step_ = 0;          // ghost fills enqueued by the current step

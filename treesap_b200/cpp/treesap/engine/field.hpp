@@ -67,7 +67,20 @@ template <class T> AMREX_GPU_HOST_DEVICE inline amrex::Array4<T> make_array4(T* 
 }
 
 inline void cuda_check(cudaError_t e, const char* what) {
-    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+        // clear the runtime's last-error slot (a failed cudaMalloc leaves its error there, and the
+        // next launch check would report it again); sticky errors stay reported by every call
+        (void)cudaGetLastError();
+        throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+/// Pending injected allocation failures of the calling host thread (ts_context_inject_fault,
+/// TS_FAULT_ALLOC): while positive, each DeviceField allocation fails as out of memory
+/// without calling cudaMalloc, and decrements it.
+inline int& alloc_faults() {
+    static thread_local int n = 0;
+    return n;
 }
 
 /// Owning, zero-initialised device buffer of one field.
@@ -75,6 +88,10 @@ template <class T> class DeviceField {
   public:
     DeviceField() = default;
     DeviceField(const int n[3], int g, int nc) : L_(Layout::make(n, g, nc, sizeof(T))) {
+        if (alloc_faults() > 0) {
+            --alloc_faults();
+            throw std::runtime_error("cudaMalloc(field): out of memory (injected)");
+        }
         cuda_check(cudaMalloc(&p_, L_.bytes()), "cudaMalloc(field)");
         cuda_check(cudaMemset(p_, 0, L_.bytes()), "cudaMemset(field)");
     }

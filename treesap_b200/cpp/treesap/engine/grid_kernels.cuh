@@ -201,6 +201,31 @@ __global__ void init_kernel(double* __restrict__ f, const Layout L, const amrex:
     }
 }
 
+/// Health check: sets *flag to 1 when any valid cell of any component is NaN or infinite.
+template <class T> __global__ void nonfinite_kernel(const T* __restrict__ f, const Layout L, int* flag) {
+    const long long ncell = (long long)L.n[0] * L.n[1] * L.n[2];
+    const long long total = ncell * L.nc;
+    bool bad = false;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = int(t / ncell);
+        const long long r = t % ncell;
+        const int i = int(r % L.n[0]), j = int((r / L.n[0]) % L.n[1]), k = int(r / ((long long)L.n[0] * L.n[1]));
+        bad = bad || !isfinite(f[L.index(i, j, k, c)]);
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
+/// Enqueues the health check of one field; `flag` (device int) must be zero beforehand.
+template <class T> void launch_nonfinite(const T* f, const Layout& L, int* flag, int sm_count, cudaStream_t stream) {
+    const long long total = L.valid_cells() * L.nc;
+    long long blocks = (total + 255) / 256;
+    if (blocks > (long long)sm_count * 16) blocks = (long long)sm_count * 16;
+    if (blocks < 1) blocks = 1;
+    nonfinite_kernel<T><<<int(blocks), 256, 0, stream>>>(f, L, flag);
+    cuda_check(cudaGetLastError(), "nonfinite_kernel launch");
+}
+
 /// Contiguous valid-cell order [comp][z][y][x] <-> field layout. dir = 0: packed -> field; 1: field -> packed.
 template <class T>
 __global__ void pack_kernel(T* __restrict__ f, const Layout L, T* __restrict__ packed, int dir) {

@@ -39,6 +39,7 @@ class SingleLevelEulerIntegrator : public SingleLevelIntegrator<PDEModelType> {
         const auto shape = Launcher::shape(L, this->sm_count(), this->tile_rows, this->z_chunks);
         const CUtensorMap& tm = this->tensor_map(state_old.data(), L, TS_F64, Launcher::box_x(), Launcher::box_y(shape));
         if (!this->dry_run_) {
+            this->take_stage_fault(sp);
             this->clock_begin(1);
             Launcher::launch(tm, this->template centre_maps<Launcher>(ep, shape), sp, model.get_rhs(), ep, shape,
                              this->stream());

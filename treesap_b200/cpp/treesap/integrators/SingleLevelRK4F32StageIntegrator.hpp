@@ -73,6 +73,7 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
             const CUtensorMap& tm =
                 this->tensor_map(state_old.data(), Lu, TS_F64, Launcher::box_x(), Launcher::box_y(shape));
             const CentreMaps cm = this->template centre_maps<Launcher>(ep, shape);
+            this->take_stage_fault(sp);
             this->clock_begin(1);
             Launcher::launch(tm, cm, sp, model.get_rhs(), ep, shape, this->stream());
             this->clock_end();
@@ -91,6 +92,7 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
             const auto shape = Launcher::shape(Lu, this->sm_count(), this->tile_rows, this->z_chunks);
             const CUtensorMap& tm = this->tensor_map(k0.data(), Lu, TS_F64, Launcher::box_x(), Launcher::box_y(shape));
             const CentreMaps cm = this->template centre_maps<Launcher>(ep, shape);
+            this->take_stage_fault(sp);
             this->clock_begin(2);
             Launcher::launch(tm, cm, sp, lin, ep, shape, this->stream());
             this->clock_end();
@@ -125,6 +127,7 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
         const auto shape = Launcher::shape(Lf, this->sm_count(), this->tile_rows, this->z_chunks);
         const CUtensorMap& tm = this->tensor_map(in.data(), Lf, TS_F32, Launcher::box_x(), Launcher::box_y(shape));
         const CentreMaps cm = this->template centre_maps<Launcher>(ep, shape);
+        this->take_stage_fault(sp);
         this->clock_begin(1 + S);
         Launcher::launch(tm, cm, sp, lin, ep, shape, this->stream());
         this->clock_end();

@@ -73,6 +73,7 @@ class SingleLevelRK4Integrator : public SingleLevelIntegrator<PDEModelType> {
         const CUtensorMap& tm = this->tensor_map(input.data(), L, TS_F64, Launcher::box_x(), Launcher::box_y(shape));
         if (this->dry_run_) return;
         const treesap_b200::CentreMaps cm = this->template centre_maps<Launcher>(ep, shape);
+        this->take_stage_fault(sp);
         this->clock_begin(1 + s);
         Launcher::launch(tm, cm, sp, model.get_rhs(), ep, shape, this->stream());
         this->clock_end();

@@ -79,6 +79,7 @@ struct IntegratorIface {
     virtual long long launches_per_step() const = 0;
     virtual void attach_clock(treesap::KernelClock* c) = 0;
     virtual void set_launch_shape(int rows, int chunks) = 0;
+    virtual bool state_is_finite() = 0;
 };
 
 /// Exposes the protected time / step counters of the front-end integrators.
@@ -142,6 +143,7 @@ template <class Integ, int NC> class Adapter final : public IntegratorIface {
     long long launches_per_step() const override { return integ_.launches_per_step(); }
     void attach_clock(treesap::KernelClock* c) override { integ_.attach_clock(c); }
     void set_launch_shape(int rows, int chunks) override { integ_.set_launch_shape(rows, chunks); }
+    bool state_is_finite() override { return integ_.state_is_finite(); }
 
   private:
     Exposed<Integ> integ_;

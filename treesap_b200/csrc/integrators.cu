@@ -168,6 +168,18 @@ ts_status ts_integrator_get_state(ts_integrator* it, double* dst, int dst_is_dev
     return guarded(it->ctx, "ts_integrator_get_state", [&] { it->impl->get_state(dst, dst_is_device != 0); });
 }
 
+ts_status ts_integrator_check_finite(ts_integrator* it) {
+    if (!it || !it->impl) return TS_ERR_INVALID_ARGUMENT;
+    bool finite = true;
+    const ts_status st = guarded(it->ctx, "ts_integrator_check_finite", [&] { finite = it->impl->state_is_finite(); });
+    if (st != TS_OK) return st;
+    if (!finite) {
+        set_error(it->ctx, "ts_integrator_check_finite: the state holds NaN or infinite values");
+        return TS_ERR_NONFINITE;
+    }
+    return TS_OK;
+}
+
 ts_status ts_integrator_step(ts_integrator* it, int nsteps) {
     if (!it || !it->impl || nsteps < 0) return TS_ERR_INVALID_ARGUMENT;
     return guarded(it->ctx, "ts_integrator_step", [&] {

@@ -20,6 +20,9 @@ struct ts_context {
     int* err = nullptr;      // device error word
     int* err_host = nullptr; // pinned mirror
     std::string last_error;
+    // pending TS_FAULT_SKIP_COPY (plane < 0: none), taken by the next stage launch
+    std::mutex fault_mutex;
+    int fault_plane = -1;
 };
 
 namespace treesap_b200 {
@@ -30,6 +33,7 @@ void set_error(ts_context* ctx, const std::string& msg) {
 
 ts_status from_cuda(ts_context* ctx, cudaError_t e, const char* what) {
     if (e == cudaSuccess) return TS_OK;
+    (void)cudaGetLastError(); // clear the last-error slot so later launch checks do not repeat it
     set_error(ctx, std::string(what) + ": " + cudaGetErrorString(e));
     return e == cudaErrorMemoryAllocation ? TS_ERR_OUT_OF_MEMORY : TS_ERR_CUDA;
 }
@@ -65,6 +69,7 @@ const char* ts_status_string(ts_status s) {
     case TS_ERR_OUT_OF_MEMORY: return "TS_ERR_OUT_OF_MEMORY";
     case TS_ERR_DEVICE: return "TS_ERR_DEVICE";
     case TS_ERR_NO_DEVICE: return "TS_ERR_NO_DEVICE";
+    case TS_ERR_NONFINITE: return "TS_ERR_NONFINITE";
     }
     return "TS_ERR_UNKNOWN";
 }
@@ -129,6 +134,39 @@ ts_status ts_context_sync(ts_context* ctx) {
         return TS_ERR_DEVICE;
     }
     return TS_OK;
+}
+
+ts_status ts_context_inject_fault(ts_context* ctx, int fault, long long arg) {
+    if (!ctx) return TS_ERR_INVALID_ARGUMENT;
+    switch (fault) {
+    case TS_FAULT_NONE: {
+        std::lock_guard<std::mutex> lock(ctx->fault_mutex);
+        ctx->fault_plane = -1;
+        alloc_faults() = 0;
+        return TS_OK;
+    }
+    case TS_FAULT_SKIP_COPY: {
+        if (arg < 0 || arg > (1 << 20)) return TS_ERR_INVALID_ARGUMENT;
+        std::lock_guard<std::mutex> lock(ctx->fault_mutex);
+        ctx->fault_plane = int(arg);
+        return TS_OK;
+    }
+    case TS_FAULT_ALLOC:
+        if (arg < 0 || arg > (1 << 20)) return TS_ERR_INVALID_ARGUMENT;
+        alloc_faults() = int(arg);
+        return TS_OK;
+    default: return TS_ERR_INVALID_ARGUMENT;
+    }
+}
+
+int ts_context_take_stage_fault(ts_context* ctx, int* plane, unsigned long long* wait_ns) {
+    if (!ctx || !plane || !wait_ns) return 0;
+    std::lock_guard<std::mutex> lock(ctx->fault_mutex);
+    if (ctx->fault_plane < 0) return 0;
+    *plane = ctx->fault_plane;
+    *wait_ns = kInjectedWaitLimitNs;
+    ctx->fault_plane = -1;
+    return 1;
 }
 
 const char* ts_context_last_error(const ts_context* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
