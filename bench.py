@@ -171,8 +171,9 @@ def cpu_baseline(desc, pulses, budget_s=15.0):
     orc = pyoracle.Oracle(which)
     _, t1, _ = orc.run(desc, 1, items=pulses)
     nsteps = int(max(1, min(10, budget_s / max(t1, 1e-3))))
-    _, secs, _ = orc.run(desc, nsteps, items=pulses)
+    state, secs, _ = orc.run(desc, nsteps, items=pulses)
     ncell = desc.n[0] * desc.n[1] * desc.n[2]
+    cpu_baseline.last = (which, nsteps, state)  # kept for the parity check of the bench line
     return {
         "value": ncell * nsteps / secs,
         "unit": UNIT,
@@ -324,6 +325,24 @@ def run_b200(args, rank, world, local_rank):
 
     cpu = cpu_baseline(c2_desc(TS_F64, N), pulses) if (rank == 0 and world == 1) else None
 
+    # parity at the benchmarked size: the GPU FP64 form against the reference build, the same
+    # steps from the same pulses as the CPU baseline's sample
+    parity = None
+    if cpu is not None:
+        from treesap_b200 import TS_INIT_GAUSSIAN, Integrator
+
+        which, nsteps, want = cpu_baseline.last
+        chk = Integrator(ctx, c2_desc(TS_F64, N))
+        chk.initialise(TS_INIT_GAUSSIAN, pulses)
+        chk.step(nsteps)
+        got = chk.get_state()
+        chk.close()
+        d = got - want
+        parity = {"against": "reference build (oracle/_ref)" if which == "ref" else "oracle port", "form": "FP64",
+                  "grid": [N, N, N], "steps": nsteps, "maxnorm_rel": float(np.abs(d).max() / np.abs(want).max()),
+                  "l2_rel": float(np.linalg.norm(d) / np.linalg.norm(want)), "tolerance": 1e-12}
+        parity["ok"] = parity["maxnorm_rel"] <= 1e-12
+
     # batched form (C4): 512 periodic instances, one persistent launch per stage, CUDA graph
     batched = None
     for r in res.values():
@@ -394,6 +413,7 @@ def run_b200(args, rank, world, local_rank):
             "roofline": roofline,
             "kernels": kernels,
             "cpu_baseline": cpu,
+            "parity": parity,
             "e2e": e2e,
             "gpu_launches": int(f32["launches"]),
             "clocks": {k: f32["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
@@ -405,6 +425,8 @@ def run_b200(args, rank, world, local_rank):
         print(json.dumps(line))
     ctx.close()
     dist.close()
+    if parity is not None and not parity["ok"]:
+        sys.exit(f"parity failure at {N}^3: GPU FP64 vs reference relative max-norm {parity['maxnorm_rel']:.3e}")
 
 
 def main():
