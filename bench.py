@@ -20,8 +20,8 @@ ts_batch_* (autotuned launch shape, one persistent launch per stage, CUDA graph)
 `adjoint`: the C5 loss + gradient through ts_adjoint_* (seconds, and the largest relative
 difference to central finite differences over 32 random directions of phi0 and of c), and
 `tensor`: C3 (192^3, 12 components) for a few steps of each form.
-For N > 1 every rank runs an independent replica (weak scaling; the z-slab halo exchange of
-a sharded domain is not part of this build).
+For N > 1 the ranks share one 256 x 256 x 256N domain, one 256^3 z slab per GPU (weak
+scaling), exchanging their boundary planes every RK4 stage over NCCL (treesap_b200/slabs.py).
 """
 from __future__ import annotations
 
@@ -63,15 +63,18 @@ def dist_env():
 class Dist:
     """Barriers and max-reductions across ranks (torch.distributed over gloo; no-op for one rank)."""
 
-    def __init__(self, world):
+    def __init__(self, world, local_rank=0):
         self.world = world
         self.dist = None
         if world > 1:
             import datetime
 
+            import torch
             import torch.distributed as dist
 
-            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+            # host tensors (barriers, timings) over gloo, device tensors (slab planes) over NCCL
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("cpu:gloo,cuda:nccl", timeout=datetime.timedelta(seconds=300))
             self.dist = dist
 
     def barrier(self):
@@ -240,6 +243,80 @@ def timed_form(ts, ctx, dist, precision, pulses, args, local_rank):
     dist.barrier()
     ms, launches = it.last_step_timing()
     return it, ms, launches, clk.summary()
+
+
+def run_sharded(args, rank, world, local_rank):
+    """N > 1: one domain of 256 x 256 x 256N cells (8 seeded pulses scaled along z) split into N
+    z slabs, one per GPU (weak scaling: every GPU holds a 256^3 slab); per RK4 stage each rank
+    exchanges its ngrow boundary planes with its neighbours over NCCL (treesap_b200.slabs)."""
+    import torch
+
+    from treesap_b200 import TS_F32_STAGE, TS_F64, TS_INIT_GAUSSIAN, Context
+    from treesap_b200.configs import c2_desc, c2_pulses
+    from treesap_b200.slabs import SlabDomain, TorchComm
+
+    dist = Dist(world, local_rank)
+    ctx = Context(local_rank)
+    ncell = N * N * N  # cells per rank
+    pulses = c2_pulses()
+    pulses[:, 5] = (pulses[:, 5] + np.arange(len(pulses)) % world) / world  # spread the pulses over the slabs
+    res = {}
+    for name, prec in (("f32", TS_F32_STAGE), ("f64", TS_F64)):
+        desc = c2_desc(prec, N)
+        desc.n[2] = N * world
+        desc.prob_hi[2] = float(world)
+        dom = SlabDomain(desc, rank, world, TorchComm(ctx.stream), ctx=ctx)
+        dom.slab.initialise(TS_INIT_GAUSSIAN, pulses)
+        dom.step(args.warmup)
+        ctx.sync()
+        dist.barrier()
+        stream = torch.cuda.ExternalStream(ctx.stream)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local_rank) as clk:
+            ev0.record(stream)
+            dom.step(args.steps)
+            ev1.record(stream)
+            ev1.synchronize()
+        dist.barrier()
+        ms = dist.max(ev0.elapsed_time(ev1))
+        res[name] = {"ms": ms, "value": world * ncell * args.steps / (ms * 1e-3), "clocks": clk.summary(), "dom": dom}
+
+    # end to end: host state in -> steps -> host state out, per rank (its slab), FP32-stage form
+    dom = res["f32"]["dom"]
+    host = dom.slab.get_state()
+    dist.barrier()
+    t0 = time.perf_counter()
+    dom.slab.set_state(host)
+    dom.step(E2E_CHUNK)
+    out = dom.slab.get_state()
+    secs = dist.max(time.perf_counter() - t0)
+    e2e = {"value": world * ncell * E2E_CHUNK / secs, "unit": UNIT, "h2d_bytes_per_step": world * host.nbytes / E2E_CHUNK,
+           "d2h_bytes_per_step": world * out.nbytes / E2E_CHUNK,
+           "call": f"per rank: slab set_state(host) -> {E2E_CHUNK} sharded steps -> get_state(host), FP32-stage form"}
+    for r in res.values():
+        r["dom"].slab.close()
+    if rank == 0:
+        f32, f64 = res["f32"], res["f64"]
+        line = {
+            "metric": METRIC, "value": f32["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": f32["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32-stage+f64-state", "data": "synthetic",
+            "config": {"workload": "C2 scalar wave, 8th-order (ngrow 4), KO 0.2, absorbing layer 16 cells, Dirichlet 0, "
+                       "RK4 dt=0.25dx, 8 seeded pulses; one 256 x 256 x 256N domain in N z slabs",
+                       "grid": [N, N, N * world], "form": "FP32-stage RK4 (FP64 state and final combination)",
+                       "l2": "no flush: every field exceeds L2 (126 MB)",
+                       "parallelism": f"z slabs x{world}, NCCL halo exchange per stage"},
+            "fp64": {"value": f64["value"], "ms_per_step": f64["ms"] / args.steps},
+            "speedup_f32_over_f64": f32["value"] / f64["value"],
+            "cpu_baseline": None, "e2e": e2e,
+            # per stage and rank: the stage kernel and one halo copy per exchanged face (the static
+            # Dirichlet ghost cells are filled once per buffer, before the timed steps)
+            "gpu_launches": args.steps * 4 * (1 + (dom.lo is not None) + (dom.hi is not None)),
+            "clocks": {k: f32["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        }
+        print(json.dumps(line))
+    ctx.close()
+    dist.close()
 
 
 def run_b200(args, rank, world, local_rank):
@@ -441,6 +518,9 @@ def main():
     rank, world, local_rank = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if world > 1:
+        run_sharded(args, rank, world, local_rank)
         return
     run_b200(args, rank, world, local_rank)
 

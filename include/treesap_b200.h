@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define TS_ABI_VERSION 1
+#define TS_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define TS_API __attribute__((visibility("default")))
@@ -140,6 +140,11 @@ typedef struct ts_wave_desc {
     int scheme;              /* ts_scheme */
     int precision;           /* ts_precision (TS_PRECISION_F32_STAGE needs TS_RK4) */
     const double* c2;        /* TS_MODEL_WAVE only: host array of c(x)^2 per valid cell, x fastest; NULL = 1 */
+    int block[3];            /* block_size (SingleLevelIntegrator.hpp:47-49): 0 < block[2] < n[2] splits the
+                              * domain into z slabs of at most block[2] planes (any scheme), whose ghost
+                              * planes are exchanged every stage; the result is bitwise the single box's.
+                              * block[0], block[1] (and 0 = the whole domain) keep one box in x and y, which
+                              * the stage kernels tile themselves. */
 } ts_wave_desc;
 
 typedef struct ts_integrator ts_integrator;
@@ -148,6 +153,38 @@ typedef struct ts_integrator ts_integrator;
  * (integrators/SingleLevelRK4Integrator.hpp:65-67, SingleLevelEulerIntegrator.hpp:51-52). */
 TS_API ts_status ts_integrator_create(ts_context* ctx, const ts_wave_desc* desc, ts_integrator** out);
 TS_API ts_status ts_integrator_destroy(ts_integrator* it);
+
+/* One z slab of a domain shared by several processes or GPUs (no counterpart in the reference,
+ * whose boxes are exchanged by AMReX's MPI FillPatch, SingleLevelIntegrator.hpp:153-163): planes
+ * [zlo, zlo + nz) of the domain `desc` (TS_MODEL_WAVE with unit speed; RK4, FP32-stage RK4 or
+ * Euler), with the
+ * lower / upper ghost planes filled by the caller's halo exchange when lo_ex / hi_ex is set
+ * (interior faces, and both end faces of a domain periodic in z), else by the ghost fill. The
+ * integrator's set/get_state and initialise act on the slab's own cells ([comp][z_slab][y][x],
+ * global coordinates); it steps through the calls below, all enqueued on the context stream:
+ *   for each stage s < ts_slab_stages():
+ *     ts_slab_prepare(s)                     (stage register step)
+ *     exchange: ts_slab_send_planes(s, face) gives the ngrow boundary planes to send to the
+ *       neighbour across `face` (0 lower, 1 upper; whole planes from component 0, `elems`
+ *       elements of `elem_size` bytes per component (8, or 4 for the FP32 stage registers),
+ *       components `comp_stride` elements apart, device memory); the planes the neighbour
+ *       sends are copied into this slab's ghost planes with ts_slab_receive_planes(s, face,
+ *       buf), buf holding ncomp blocks of `elems` elements (device memory)
+ *     ts_slab_fill(s)                        (every other ghost cell)
+ *     ts_slab_launch(s)                      (the fused stage kernel)
+ *   ts_slab_finish()                         (time, step count, state swap)
+ * Every process must take the same stages in the same order; the neighbour's planes for stage s
+ * are those of its stage-s register after its ts_slab_prepare(s). */
+TS_API ts_status ts_integrator_create_slab(ts_context* ctx, const ts_wave_desc* desc, int zlo, int nz, int lo_ex,
+                                           int hi_ex, ts_integrator** out);
+TS_API int ts_slab_stages(ts_integrator* it);
+TS_API ts_status ts_slab_prepare(ts_integrator* it, int stage);
+TS_API ts_status ts_slab_send_planes(ts_integrator* it, int stage, int face, void** ptr, long long* elems,
+                                     long long* comp_stride, int* elem_size);
+TS_API ts_status ts_slab_receive_planes(ts_integrator* it, int stage, int face, const void* buf);
+TS_API ts_status ts_slab_fill(ts_integrator* it, int stage);
+TS_API ts_status ts_slab_launch(ts_integrator* it, int stage);
+TS_API ts_status ts_slab_finish(ts_integrator* it);
 TS_API int ts_integrator_ncomp(const ts_integrator* it);
 
 /* initialise() (Integrator.hpp:75-78, SingleLevelIntegrator.hpp:75-93): evaluates the

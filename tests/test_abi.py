@@ -35,7 +35,7 @@ def test_build_targets_sm100a_only():
 
 def test_status_strings_and_version():
     lib = tsb.lib()
-    assert lib.ts_abi_version() == 1
+    assert lib.ts_abi_version() == 2
     assert lib.ts_status_string(0) == b"TS_OK"
     assert lib.ts_status_string(6) == b"TS_ERR_NO_DEVICE"
 

@@ -85,6 +85,7 @@ class WaveDesc(C.Structure):
         ("scheme", C.c_int),
         ("precision", C.c_int),
         ("c2", C.c_void_p),
+        ("block", C.c_int * 3),
     ]
 
     def ncomp(self) -> int:
@@ -150,6 +151,14 @@ def lib() -> C.CDLL:
         "ts_integrator_state_field": (i, [vp, C.POINTER(vp), C.POINTER(FieldLayout)]),
         "ts_integrator_use_graph": (i, [vp, i]),
         "ts_integrator_check_finite": (i, [vp]),
+        "ts_integrator_create_slab": (i, [vp, C.POINTER(WaveDesc), i, i, i, i, C.POINTER(vp)]),
+        "ts_slab_stages": (i, [vp]),
+        "ts_slab_prepare": (i, [vp, i]),
+        "ts_slab_send_planes": (i, [vp, i, i, C.POINTER(vp), C.POINTER(ll), C.POINTER(ll), C.POINTER(i)]),
+        "ts_slab_receive_planes": (i, [vp, i, i, vp]),
+        "ts_slab_fill": (i, [vp, i]),
+        "ts_slab_launch": (i, [vp, i]),
+        "ts_slab_finish": (i, [vp]),
         "ts_integrator_last_step_timing": (i, [vp, C.POINTER(d), C.POINTER(ll)]),
         "ts_integrator_profile": (i, [vp, i, i, C.POINTER(ll), C.POINTER(d)]),
         "ts_integrator_set_launch_shape": (i, [vp, i, i]),

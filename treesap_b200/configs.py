@@ -38,6 +38,7 @@ def wave_desc(
     prob_lo=(0.0, 0.0, 0.0),
     prob_hi=(1.0, 1.0, 1.0),
     model: int = TS_MODEL_WAVE,
+    block=(0, 0, 0),
 ) -> WaveDesc:
     d = WaveDesc()
     n = (n, n, n) if np.isscalar(n) else tuple(n)
@@ -59,6 +60,7 @@ def wave_desc(
     d.scheme = scheme
     d.precision = precision
     d.c2 = None
+    d.block[:] = list(block)
     return d
 
 

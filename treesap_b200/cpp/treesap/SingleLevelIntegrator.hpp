@@ -12,6 +12,7 @@
 #include <AMReX.H>
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <optional>
 #include <stdexcept>
 #include <vector>
@@ -138,9 +139,16 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
     using Field = treesap_b200::DeviceField<amrex::Real>;
 
   public:
-    SingleLevelIntegrator(PDEModelType model_, const amrex::IntVect& block_size, ts_context* ctx_ = nullptr)
+    /// `slab` / `slab_depth`: this integrator owns planes [slab.zoff, slab.zoff + slab_depth) of the
+    /// model's domain (a z slab, see ZSlabDomain.hpp); the default is the whole domain.
+    SingleLevelIntegrator(PDEModelType model_, const amrex::IntVect& block_size, ts_context* ctx_ = nullptr,
+                          treesap_b200::SlabZ slab = {}, int slab_depth = 0)
         : Base(std::move(model_)), ctx(ctx_ ? ctx_ : treesap_b200::default_context()),
-          geom(model.get_geometry().data()), state_old(extent(), ngrow, ncomp), state_new(extent(), ngrow, ncomp) {
+          geom(model.get_geometry().data()), slab_(slab), slab_depth_(slab_depth), state_old(extent(), ngrow, ncomp),
+          state_new(extent(), ngrow, ncomp) {
+        if (slab_.nz > 0 && (slab_depth_ < ngrow || slab_.zoff < 0 || slab_.zoff + slab_depth_ > slab_.nz ||
+                             slab_.nz != geom.domain.length(2)))
+            throw std::invalid_argument("z slab outside the domain or thinner than the ghost width");
         for (int d = 0; d < 3; ++d) {
             if (block_size[d] < 1) throw std::invalid_argument("block_size must be positive");
             if (geom.domain.length(d) < ngrow) throw std::invalid_argument("domain smaller than the ghost width");
@@ -176,7 +184,7 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
         long long blocks = (ncell + 255) / 256;
         if (blocks > 32LL * sm_count()) blocks = 32LL * sm_count();
         treesap_b200::init_kernel<ncomp, InitType>
-            <<<int(blocks), 256, 0, stream()>>>(state_old.data(), L, geom, model.get_init());
+            <<<int(blocks), 256, 0, stream()>>>(state_old.data(), L, geom, model.get_init(), slab_.zoff);
         treesap_b200::cuda_check(cudaGetLastError(), "init_kernel launch");
         steps = 0;
         time = 0.0;
@@ -290,15 +298,39 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
     void count_fill() { ++fills_this_step_; }
 
     /// Ghost fill of an FP64 field with the model's BC functor (SingleLevelIntegrator.hpp:153-163).
+    /// For a z slab the halo hook first copies the neighbouring slabs' boundary planes into the
+    /// exchange ghost planes; the ghost fill then completes every other ghost cell.
     void FillPatch(Field& f, amrex::Real time_) {
         ScopedTimer timer("Integrator::FillPatch()");
         if (dry_run_) return;
+        halo(f);
         if (!ghost_fill_needed(f.data())) return;
         count_fill();
         clock_begin(0);
         treesap_b200::launch_ghost_fill(f.data(), f.layout(), geom, model.get_bc(), bc_recs_dev, time_,
-                                        treesap_b200::GhostMode::Functor, sm_count(), stream());
+                                        treesap_b200::GhostMode::Functor, sm_count(), stream(), slab_);
         clock_end();
+    }
+
+  public:
+    /// Where this integrator sits in a z-slab decomposition (zoff = global z of its plane 0).
+    const treesap_b200::SlabZ& slab() const { return slab_; }
+    /// A stage register of any element type: its data and layout.
+    struct FieldRef {
+        void* data;
+        treesap_b200::Layout L;
+    };
+    /// Called before every ghost fill with the field whose exchange ghost planes must be filled
+    /// from the neighbouring slabs (the same stage register of every slab).
+    using HaloHook = std::function<void(const FieldRef&)>;
+    void set_halo_hook(HaloHook hook) { halo_hook_ = std::move(hook); }
+
+  protected:
+    /// The halo exchange of field f (when this integrator is a slab with exchange faces).
+    template <class T> void halo(treesap_b200::DeviceField<T>& f) {
+        if (!halo_hook_ || dry_run_) return;
+        halo_hook_(FieldRef{f.data(), f.layout()});
+        count_fill();
     }
 
     /// Applies a pending injected stage fault of the context (ts_context_inject_fault,
@@ -330,8 +362,10 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
         for (int d = 0; d < 3; ++d) n[d] = g.Domain().length(d);
         return n;
     }
+    /// Cells of this integrator's box: the domain, or the z slab.
     const int* extent() {
         extent_of(model.get_geometry(), extent_buf);
+        if (slab_.nz > 0) extent_buf[2] = slab_depth_;
         return extent_buf;
     }
 
@@ -345,6 +379,9 @@ class SingleLevelIntegrator : public Integrator<PDEModelType> {
     ts_context* ctx;
     int extent_buf[3] = {0, 0, 0};
     amrex::GeometryData geom;
+    treesap_b200::SlabZ slab_; // z-slab placement (default: the whole domain)
+    int slab_depth_ = 0;
+    HaloHook halo_hook_;
     Field state_old;
     Field state_new;
     amrex::BCRec* bc_recs_dev = nullptr;

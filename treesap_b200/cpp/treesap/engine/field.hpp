@@ -60,11 +60,22 @@ struct Layout {
     }
 };
 
-/// Plain (view-less) Array4 over a field, with AMReX's index convention.
-template <class T> AMREX_GPU_HOST_DEVICE inline amrex::Array4<T> make_array4(T* base, const Layout& L) {
-    return amrex::Array4<T>(base, L.px, L.px * L.py, L.comp_stride(), amrex::Dim3{-L.xoff, -L.g, -L.g},
-                            amrex::Dim3{int(L.px) - L.xoff, L.n[1] + L.g, L.n[2] + L.g}, L.nc);
+/// Plain (view-less) Array4 over a field, with AMReX's index convention. `zoff`: global z index
+/// of the field's plane 0 (a z slab of a larger domain), so that the Array4 takes global indices.
+template <class T> AMREX_GPU_HOST_DEVICE inline amrex::Array4<T> make_array4(T* base, const Layout& L, int zoff = 0) {
+    return amrex::Array4<T>(base, L.px, L.px * L.py, L.comp_stride(), amrex::Dim3{-L.xoff, -L.g, zoff - L.g},
+                            amrex::Dim3{int(L.px) - L.xoff, L.n[1] + L.g, zoff + L.n[2] + L.g}, L.nc);
 }
+
+/// Where a field sits in a domain decomposed into z slabs: its plane 0 is global plane `zoff`
+/// of a domain `nz` planes deep, and its lower / upper ghost planes are filled by a halo
+/// exchange with the neighbouring slabs (`lo_ex` / `hi_ex`) rather than by the ghost fill.
+/// The default (nz = 0) is a single box: the field is the whole domain.
+struct SlabZ {
+    int zoff = 0;
+    int nz = 0;
+    int lo_ex = 0, hi_ex = 0;
+};
 
 inline void cuda_check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) {

@@ -99,40 +99,46 @@ AMREX_GPU_HOST_DEVICE inline void ghost_coords(const Layout& L, long long t, int
 }
 
 /// Fills ghost cell number t of field f (slab enumeration of ghost_coords).
+/// For a z slab (sz.nz > 0) the ghost cells of exchange planes (sz.lo_ex / sz.hi_ex) are left to
+/// the halo exchange, and the domain tests and the BC functor use global z (local + sz.zoff);
+/// the periodic source of every other ghost cell lies in the slab's own planes.
 template <class T, class BC>
 __device__ __forceinline__ void ghost_fill_cell(T* __restrict__ f, const Layout& L, const amrex::GeometryData& geom,
                                                 const BC& bc, const amrex::BCRec* bcr, double time, int mode,
-                                                long long t) {
+                                                long long t, const SlabZ& sz = SlabZ{}) {
     int i, j, k;
     ghost_coords(L, t, i, j, k);
-    int s[3] = {i, j, k};
+    if ((k < 0 && sz.lo_ex) || (k >= L.n[2] && sz.hi_ex)) return; // filled by the halo exchange
+    const int nzg = sz.nz > 0 ? sz.nz : L.n[2];
+    const int n[3] = {L.n[0], L.n[1], nzg};
+    int s[3] = {i, j, k + sz.zoff};
     bool inside = true;
     for (int d = 0; d < 3; ++d) {
-        if (geom.is_periodic[d]) s[d] = ((s[d] % L.n[d]) + L.n[d]) % L.n[d];
-        if (s[d] < 0 || s[d] >= L.n[d]) inside = false;
+        if (geom.is_periodic[d]) s[d] = ((s[d] % n[d]) + n[d]) % n[d];
+        if (s[d] < 0 || s[d] >= n[d]) inside = false;
     }
     const long long cs = L.comp_stride();
     if (inside) {
-        const long long dst = L.index(i, j, k, 0), src = L.index(s[0], s[1], s[2], 0);
+        const long long dst = L.index(i, j, k, 0), src = L.index(s[0], s[1], s[2] - sz.zoff, 0);
         for (int c = 0; c < L.nc; ++c) f[dst + c * cs] = f[src + c * cs];
     } else if (mode == int(GhostMode::Homogeneous)) {
         const long long dst = L.index(i, j, k, 0);
         for (int c = 0; c < L.nc; ++c) f[dst + c * cs] = T(0);
     } else if (mode == int(GhostMode::Functor)) {
         if constexpr (std::is_same_v<T, amrex::Real>) {
-            const amrex::Array4<amrex::Real> dest = make_array4(f, L);
-            bc(amrex::IntVect{i, j, k}, dest, 0, L.nc, geom, time, bcr, 0, 0);
+            const amrex::Array4<amrex::Real> dest = make_array4(f, L, sz.zoff);
+            bc(amrex::IntVect{i, j, k + sz.zoff}, dest, 0, L.nc, geom, time, bcr, 0, 0);
         }
     }
 }
 
 template <class T, class BC>
 __global__ void ghost_fill_kernel(T* __restrict__ f, const Layout L, const amrex::GeometryData geom, const BC bc,
-                                  const amrex::BCRec* bcr, double time, int mode) {
+                                  const amrex::BCRec* bcr, double time, int mode, const SlabZ sz) {
     const long long total = ghost_count(L).total();
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x)
-        ghost_fill_cell(f, L, geom, bc, bcr, time, mode, t);
+        ghost_fill_cell(f, L, geom, bc, bcr, time, mode, t, sz);
 }
 
 /// One field of a batched ghost fill.
@@ -175,27 +181,61 @@ __global__ void __launch_bounds__(256) batch_ghost_fill_kernel(const GhostEntry<
 
 template <class T, class BC>
 void launch_ghost_fill(T* f, const Layout& L, const amrex::GeometryData& geom, const BC& bc, const amrex::BCRec* bcr,
-                       double time, GhostMode mode, int sm_count, cudaStream_t stream) {
+                       double time, GhostMode mode, int sm_count, cudaStream_t stream, const SlabZ& sz = SlabZ{}) {
     const long long total = ghost_count(L).total();
     if (total == 0) return;
     const int threads = 256;
     long long blocks = (total + threads - 1) / threads;
     const long long cap = (long long)sm_count * 16;
     if (blocks > cap) blocks = cap;
-    ghost_fill_kernel<T, BC><<<int(blocks), threads, 0, stream>>>(f, L, geom, bc, bcr, time, int(mode));
+    ghost_fill_kernel<T, BC><<<int(blocks), threads, 0, stream>>>(f, L, geom, bc, bcr, time, int(mode), sz);
     cuda_check(cudaGetLastError(), "ghost_fill_kernel launch");
 }
 
+/// Halo exchange between z slabs: copies the valid x-y region of `np` planes, all components,
+/// into planes [kd0, kd0 + np) of field `dst` (layout Ld) from a source with the same x-y
+/// geometry (px, py, xoff, ghost width): element (i, j, p, c) of the source is at
+/// src[c * src_cs + p * px * py + (j + g) * px + i + xoff] (src: a neighbour field from its
+/// plane ks0 on, or a staging buffer of whole planes received from another GPU).
+template <class T>
+__global__ void halo_copy_kernel(T* __restrict__ dst, const Layout Ld, int kd0, const T* __restrict__ src,
+                                 long long src_cs, int np) {
+    const long long row = Ld.n[0], rows = Ld.n[1], plane = Ld.px * Ld.py;
+    const long long total = (long long)Ld.nc * np * rows * row;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = int(t % row);
+        long long r = t / row;
+        const int j = int(r % rows);
+        r /= rows;
+        const int p = int(r % np), c = int(r / np);
+        dst[Ld.index(i, j, kd0 + p, c)] = src[c * src_cs + p * plane + (long long)(j + Ld.g) * Ld.px + i + Ld.xoff];
+    }
+}
+
+template <class T>
+void launch_halo_copy(T* dst, const Layout& Ld, int kd0, const T* src, long long src_cs, int np, int sm_count,
+                      cudaStream_t stream) {
+    const long long total = (long long)Ld.nc * np * Ld.n[1] * Ld.n[0];
+    if (total == 0) return;
+    long long blocks = (total + 255) / 256;
+    if (blocks > (long long)sm_count * 16) blocks = (long long)sm_count * 16;
+    halo_copy_kernel<T><<<int(blocks), 256, 0, stream>>>(dst, Ld, kd0, src, src_cs, np);
+    cuda_check(cudaGetLastError(), "halo_copy_kernel launch");
+}
+
 /// initialise(): state(i,j,k,c) = init<c>(lo + (i + 1/2) dx, ...) (SingleLevelIntegrator.hpp:84-92).
+/// `zoff`: global z index of the field's plane 0 (z slabs).
 template <int NC, class Init>
-__global__ void init_kernel(double* __restrict__ f, const Layout L, const amrex::GeometryData geom, const Init init) {
+__global__ void init_kernel(double* __restrict__ f, const Layout L, const amrex::GeometryData geom, const Init init,
+                            int zoff = 0) {
     const long long ncell = (long long)L.n[0] * L.n[1] * L.n[2];
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ncell;
          t += (long long)gridDim.x * blockDim.x) {
         const int i = int(t % L.n[0]), j = int((t / L.n[0]) % L.n[1]), k = int(t / ((long long)L.n[0] * L.n[1]));
         const double x = geom.prob_lo[0] + (i + 0.5) * geom.dx[0];
         const double y = geom.prob_lo[1] + (j + 0.5) * geom.dx[1];
-        const double z = geom.prob_lo[2] + (k + 0.5) * geom.dx[2];
+        const double z = geom.prob_lo[2] + (k + zoff + 0.5) * geom.dx[2];
         const long long o = L.index(i, j, k, 0), cs = L.comp_stride();
         treesap::static_for<NC>([&]<int c>() { f[o + c * cs] = init.template operator()<c>(x, y, z); });
     }

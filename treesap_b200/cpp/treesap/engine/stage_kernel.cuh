@@ -163,6 +163,7 @@ template <typename T> struct StageParams {
     int* err;                 // device error word
     unsigned long long wait_ns = kWaitLimitNs; // bound of every mbarrier wait of the launch
     int skip_plane = -1; // injected fault: the producer skips the copy of this plane of every item
+    int zoff = 0;        // global z index of the input's plane 0 (a z slab of a larger domain)
 };
 
 /// TMA descriptors of the centre-operand fields (box TX x ty CY x 1 x NC) and the storage
@@ -247,8 +248,8 @@ __device__ __forceinline__ void eval_components(const RHS& f, T (&kv)[NC], const
 template <class RHS, class T, int NC>
 __device__ __forceinline__ void eval_cell(const RHS& f, T (&kv)[NC], const amrex::StencilView<T>& view, const T* in,
                                           const Layout& L, const amrex::IntVect& idx, double time,
-                                          const amrex::GeometryData& geom) {
-    amrex::Array4<const T> arr = make_array4<const T>(in, L);
+                                          const amrex::GeometryData& geom, int zoff) {
+    amrex::Array4<const T> arr = make_array4<const T>(in, L, zoff);
     arr.view = &view;
     typename RHS::Workspace ws{};
     eval_components(f, kv, idx, time, arr, geom, ws, std::make_integer_sequence<int, NC>{});
@@ -471,6 +472,7 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
         const double time = spr.time;
         const T* const in = spr.in;
         const unsigned long long wl = spr.wait_ns;
+        const int zo = spr.zoff; // the functor sees global z
         const typename Epi::Params epl = src.epi(b.inst);
 
         const int NP = (b.z1 - b.z0) + 2 * ZH;
@@ -619,7 +621,7 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
                                                         L.comp_stride(),
                                                         i0 + e,
                                                         j0 + r,
-                                                        z,
+                                                        z + zo,
                                                         BX,
                                                         PNS,
                                                         ZH,
@@ -650,15 +652,16 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
                         // neighbouring cells can share vector loads
 #pragma unroll
                         for (int e = 0; e < CX; ++e)
-                            eval_cell(f, kv[u][r][e], view[e], in, L, amrex::IntVect{i0 + e, j0 + r, z}, time, geom);
+                            eval_cell(f, kv[u][r][e], view[e], in, L, amrex::IntVect{i0 + e, j0 + r, z + zo}, time,
+                                      geom, zo);
                     } else {
 #pragma unroll
                         for (int e = 0; e < CX; ++e) {
 #pragma unroll
                             for (int c = 0; c < NC; ++c) kv[u][r][e][c] = T(0);
                             if ((U == 1 || it + u < NP) && act[r][e])
-                                eval_cell(f, kv[u][r][e], view[e], in, L, amrex::IntVect{i0 + e, j0 + r, z}, time,
-                                          geom);
+                                eval_cell(f, kv[u][r][e], view[e], in, L, amrex::IntVect{i0 + e, j0 + r, z + zo}, time,
+                                          geom, zo);
                         }
                     }
                 }

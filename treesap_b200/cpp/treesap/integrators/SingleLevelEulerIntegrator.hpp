@@ -22,8 +22,25 @@ class SingleLevelEulerIntegrator : public SingleLevelIntegrator<PDEModelType> {
   public:
     using Tile = typename detail::DefaultTile<double, ngrow, ncomp>::type;
 
-    SingleLevelEulerIntegrator(PDEModelType model_, const amrex::IntVect& block_size, ts_context* ctx_ = nullptr)
-        : Base(std::move(model_), block_size, ctx_) {}
+    SingleLevelEulerIntegrator(PDEModelType model_, const amrex::IntVect& block_size, ts_context* ctx_ = nullptr,
+                               treesap_b200::SlabZ slab = {}, int slab_depth = 0)
+        : Base(std::move(model_), block_size, ctx_, slab, slab_depth) {}
+
+    // ---- stage-level stepping for z slabs (ZSlabDomain.hpp): one stage reading the state.
+    static constexpr int kStages = 1;
+    void stage_prepare(int) {}
+    typename Base::Field& stage_input(int) { return state_old; }
+    typename Base::FieldRef stage_ref(int) { return {state_old.data(), state_old.layout()}; }
+    void stage_fill(int, amrex::Real) {
+        this->fills_this_step_ = 0;
+        this->FillPatch(state_old, time);
+    }
+    void stage_launch(int, amrex::Real dt) { computeNewState(dt); }
+    void stage_finish(amrex::Real dt) {
+        ++this->steps;
+        time += dt;
+        swap(state_old, state_new);
+    }
 
   protected:
     amrex::Real computeNewState(amrex::Real delta_time) override {
@@ -34,6 +51,7 @@ class SingleLevelEulerIntegrator : public SingleLevelIntegrator<PDEModelType> {
         sp.geom = geom;
         sp.time = time;
         sp.err = ts_context_error_word(this->ctx);
+        sp.zoff = this->slab().zoff;
         treesap_b200::EpiEuler::Params ep{state_new.data(), L, delta_time};
         using Launcher = treesap_b200::StageLauncher<Tile, RHSType, treesap_b200::EpiEuler>;
         const auto shape = Launcher::shape(L, this->sm_count(), this->tile_rows, this->z_chunks);

@@ -48,18 +48,71 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
     using Tile64 = typename detail::DefaultTile<double, ngrow, ncomp>::type;
     using Tile32 = typename detail::DefaultTile<float, ngrow, ncomp>::type;
 
-    SingleLevelRK4F32StageIntegrator(PDEModelType model_, const amrex::IntVect& block_size, ts_context* ctx_ = nullptr)
-        : Base(std::move(model_), block_size, ctx_), k0(this->extent(), ngrow, ncomp),
+    SingleLevelRK4F32StageIntegrator(PDEModelType model_, const amrex::IntVect& block_size, ts_context* ctx_ = nullptr,
+                                     treesap_b200::SlabZ slab = {}, int slab_depth = 0)
+        : Base(std::move(model_), block_size, ctx_, slab, slab_depth), k0(this->extent(), ngrow, ncomp),
           d1(this->extent(), ngrow, ncomp), d2(this->extent(), ngrow, ncomp), lin(linear_part_of(model.get_rhs())) {}
+
+    // ---- stage-level stepping for z slabs (ZSlabDomain.hpp, ts_slab_*): the inputs of the four
+    // stages are u, k0 (FP64) and d1, d2 (FP32).
+    static constexpr int kStages = 4;
+    void stage_prepare(int) {}
+    typename Base::FieldRef stage_ref(int s) {
+        switch (s) {
+        case 0: return {state_old.data(), state_old.layout()};
+        case 1: return {k0.data(), k0.layout()};
+        case 2: return {d1.data(), d1.layout()};
+        default: return {d2.data(), d2.layout()};
+        }
+    }
+    void stage_fill(int s, amrex::Real) {
+        switch (s) {
+        case 0:
+            this->fills_this_step_ = 0;
+            this->FillPatch(state_old, time);
+            break;
+        case 1: fill_increment(k0); break;
+        case 2: fill_increment(d1); break;
+        default: fill_increment(d2); break;
+        }
+    }
+    void stage_launch(int s, amrex::Real dt) {
+        if (this->dry_run_) return;
+        int* err = ts_context_error_word(this->ctx);
+        switch (s) {
+        case 0: launch_s0(dt, err); break;
+        case 1: launch_s1(dt, err); break;
+        case 2: lin_stage<2>(d1, d2, float(0.5 * dt), dt, err); break;
+        default: lin_stage<3>(d2, d2, float(dt), dt, err); break;
+        }
+    }
+    void stage_finish(amrex::Real dt) {
+        this->launches_per_step_ = 4 + this->fills_this_step_;
+        ++this->steps;
+        time += dt;
+        swap(state_old, state_new);
+    }
 
   protected:
     amrex::Real computeNewState(amrex::Real dt) override {
-        using namespace treesap_b200;
         if (this->dry_run_) return dt;
-        const Layout& Lu = state_old.layout();
-        const Layout& Lf = d1.layout();
         int* err = ts_context_error_word(this->ctx);
-        // stage 0: k0 = F(u), u_p = u + dt k0 (into state_new)
+        launch_s0(dt, err);
+        fill_increment(k0);
+        launch_s1(dt, err);
+        fill_increment(d1);
+        lin_stage<2>(d1, d2, float(0.5 * dt), dt, err);
+        fill_increment(d2);
+        lin_stage<3>(d2, d2, float(dt), dt, err);
+        this->launches_per_step_ = 4 + this->fills_this_step_;
+        return dt;
+    }
+
+  private:
+    /// stage 0: k0 = F(u), u_p = u + dt k0 (into state_new)
+    void launch_s0(amrex::Real dt, int* err) {
+        using namespace treesap_b200;
+        const Layout& Lu = state_old.layout();
         {
             StageParams<double> sp{};
             sp.in = state_old.data();
@@ -67,6 +120,7 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
             sp.geom = geom;
             sp.time = time;
             sp.err = err;
+            sp.zoff = this->slab().zoff;
             EpiF32S0::Params ep{k0.data(), state_new.data(), Lu, dt};
             using Launcher = StageLauncher<Tile64, RHSType, EpiF32S0>;
             const auto shape = Launcher::shape(Lu, this->sm_count(), this->tile_rows, this->z_chunks);
@@ -78,8 +132,12 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
             Launcher::launch(tm, cm, sp, model.get_rhs(), ep, shape, this->stream());
             this->clock_end();
         }
-        fill_increment(k0);
-        // stage 1: d1 = dt/2 L k0 (FP64 stencil)
+    }
+    /// stage 1: d1 = dt/2 L k0 (FP64 stencil)
+    void launch_s1(amrex::Real dt, int* err) {
+        using namespace treesap_b200;
+        const Layout& Lu = state_old.layout();
+        const Layout& Lf = d1.layout();
         {
             StageParams<double> sp{};
             sp.in = k0.data();
@@ -87,6 +145,7 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
             sp.geom = geom;
             sp.time = time;
             sp.err = err;
+            sp.zoff = this->slab().zoff;
             EpiF32S1::Params ep{d1.data(), Lf, 0.5 * dt};
             using Launcher = StageLauncher<Tile64, LinearRHS, EpiF32S1>;
             const auto shape = Launcher::shape(Lu, this->sm_count(), this->tile_rows, this->z_chunks);
@@ -97,15 +156,8 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
             Launcher::launch(tm, cm, sp, lin, ep, shape, this->stream());
             this->clock_end();
         }
-        fill_increment(d1);
-        lin_stage<2>(d1, d2, float(0.5 * dt), dt, err);
-        fill_increment(d2);
-        lin_stage<3>(d2, d2, float(dt), dt, err);
-        this->launches_per_step_ = 4 + this->fills_this_step_;
-        return dt;
     }
 
-  private:
     template <int S> void lin_stage(const FieldF& in, FieldF& out, float a_dt, double dt, int* err) {
         using namespace treesap_b200;
         const Layout& Lf = in.layout();
@@ -115,6 +167,7 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
         sp.geom = geom;
         sp.time = time;
         sp.err = err;
+        sp.zoff = this->slab().zoff;
         typename EpiF32Lin<S>::Params ep{};
         ep.d_out = (S < 3) ? out.data() : nullptr;
         ep.d1 = d1.data();
@@ -134,11 +187,14 @@ class SingleLevelRK4F32StageIntegrator : public SingleLevelIntegrator<PDEModelTy
     }
 
     template <class F> void fill_increment(F& f) {
+        if (this->dry_run_) return;
+        this->halo(f);
         if (!this->ghost_fill_needed(f.data())) return;
         this->count_fill();
         this->clock_begin(0);
         treesap_b200::launch_ghost_fill(f.data(), f.layout(), geom, model.get_bc(), this->bc_recs_dev, time,
-                                        treesap_b200::GhostMode::Homogeneous, this->sm_count(), this->stream());
+                                        treesap_b200::GhostMode::Homogeneous, this->sm_count(), this->stream(),
+                                        this->slab());
         this->clock_end();
     }
 

@@ -31,8 +31,9 @@ class SingleLevelRK4Integrator : public SingleLevelIntegrator<PDEModelType> {
   public:
     using Tile = typename detail::DefaultTile<double, ngrow, ncomp>::type;
 
-    SingleLevelRK4Integrator(PDEModelType model_, const amrex::IntVect& block_size, ts_context* ctx_ = nullptr)
-        : Base(std::move(model_), block_size, ctx_), arg(this->extent(), ngrow, ncomp),
+    SingleLevelRK4Integrator(PDEModelType model_, const amrex::IntVect& block_size, ts_context* ctx_ = nullptr,
+                             treesap_b200::SlabZ slab = {}, int slab_depth = 0)
+        : Base(std::move(model_), block_size, ctx_, slab, slab_depth), arg(this->extent(), ngrow, ncomp),
           arg_next(this->extent(), ngrow, ncomp) {}
 
   private:
@@ -50,15 +51,52 @@ class SingleLevelRK4Integrator : public SingleLevelIntegrator<PDEModelType> {
         return delta_time;
     }
 
+    // ---- stage-level stepping, for domains split into z slabs (ZSlabDomain.hpp): every slab
+    // takes stage s's register step, then every slab its ghost fill (whose halo hook reads the
+    // neighbours' stage-s input), then every slab its stage kernel.
+    static constexpr int kStages = stage_count;
+    /// Stage s > 0: the register swap that makes the previous stage's output the stage input.
+    void stage_prepare(int s) {
+        if (s > 0) swap(arg_next, arg);
+    }
+    /// The field stage s reads (valid after stage_prepare(s)).
+    Field& stage_input(int s) { return s == 0 ? state_old : arg; }
+    typename Base::FieldRef stage_ref(int s) { return {stage_input(s).data(), stage_input(s).layout()}; }
+    /// Ghost fill (with the halo hook) of stage s's input at the stage time.
+    void stage_fill(int s, amrex::Real dt) {
+        if (s == 0) this->fills_this_step_ = 0;
+        FillPatch(stage_input(s), time + dt * a_fraction[s]);
+    }
+    /// The fused stage kernel of stage s.
+    void stage_launch(int s, amrex::Real dt) {
+        switch (s) {
+        case 0: launch_stage<0>(dt); break;
+        case 1: launch_stage<1>(dt); break;
+        case 2: launch_stage<2>(dt); break;
+        default: launch_stage<3>(dt); break;
+        }
+    }
+    /// After stage 3: the step's bookkeeping (counters, state swap).
+    void stage_finish(amrex::Real dt) {
+        this->launches_per_step_ = 4 + this->fills_this_step_;
+        ++steps;
+        time += dt;
+        swap(state_old, state_new);
+    }
+
   private:
     template <int s> void run_stage(amrex::Real dt) {
+        if constexpr (s > 0) {
+            stage_prepare(s);
+            FillPatch(arg, time + dt * a_fraction[s]);
+        }
+        launch_stage<s>(dt);
+    }
+
+    template <int s> void launch_stage(amrex::Real dt) {
         const double a_next = dt * a_fraction[(s + 1) % stage_count];
         const double time_arg = time + dt * a_fraction[s];
         const double b = dt * b_fraction[s];
-        if constexpr (s > 0) {
-            swap(arg_next, arg);
-            FillPatch(arg, time_arg);
-        }
         const Field& input = (s == 0) ? state_old : arg;
         const auto& L = input.layout();
         treesap_b200::StageParams<double> sp{};
@@ -67,6 +105,7 @@ class SingleLevelRK4Integrator : public SingleLevelIntegrator<PDEModelType> {
         sp.geom = geom;
         sp.time = time_arg;
         sp.err = ts_context_error_word(this->ctx);
+        sp.zoff = this->slab().zoff;
         typename treesap_b200::EpiRK4<s>::Params ep{state_new.data(), arg_next.data(), state_old.data(), L, b, a_next};
         using Launcher = treesap_b200::StageLauncher<Tile, RHSType, treesap_b200::EpiRK4<s>>;
         const auto shape = Launcher::shape(L, this->sm_count(), this->tile_rows, this->z_chunks);

@@ -15,6 +15,7 @@
 #include "integrators/SingleLevelEulerIntegrator.hpp"
 #include "integrators/SingleLevelRK4F32StageIntegrator.hpp"
 #include "integrators/SingleLevelRK4Integrator.hpp"
+#include "integrators/ZSlabDomain.hpp"
 #include "pde-model/ABLPDEModel.hpp"
 #include "pde-model/PDEModel.hpp"
 #include "pde-model/bcs/DirichletBC.hpp"
@@ -62,8 +63,37 @@ template <int NC> struct TableInit {
     }
 };
 
+/// Stage-level operations of one z slab of a domain shared by several processes (ts_slab_*).
+struct SlabOps {
+    virtual ~SlabOps() = default;
+    virtual int stages() const = 0;
+    virtual void prepare(int s) = 0;
+    /// The ngrow boundary planes sent to the neighbour across `face` (0 lower, 1 upper): whole
+    /// planes from component 0, `elems` elements of `esize` bytes per component, components `cs`
+    /// elements apart.
+    virtual void send_planes(int s, int face, void** ptr, long long* elems, long long* cs, int* esize) = 0;
+    /// Copies received planes (ncomp blocks of `elems` elements) into the ghost planes of `face`.
+    virtual void receive_planes(int s, int face, const void* buf) = 0;
+    virtual void fill(int s) = 0;
+    virtual void launch(int s) = 0;
+    virtual void finish() = 0;
+};
+
+/// A slab request for the next model built on this host thread (ts_integrator_create_slab):
+/// make_for_model then builds the slab's integrator instead of a whole-domain one.
+struct SlabRequest {
+    bool active = false;
+    SlabZ sz{};
+    int depth = 0;
+};
+inline SlabRequest& slab_request() {
+    static thread_local SlabRequest r;
+    return r;
+}
+
 struct IntegratorIface {
     virtual ~IntegratorIface() = default;
+    virtual SlabOps* slab_ops() { return nullptr; }
     virtual int ncomp() const = 0;
     virtual void initialise(int kind, int nitems, const double* items) = 0;
     /// Expression initial condition: one expression of x, y, z per component.
@@ -151,6 +181,179 @@ template <class Integ, int NC> class Adapter final : public IntegratorIface {
     std::size_t table_cap_;
 };
 
+/// A domain split into z slabs (ts_wave_desc.block[2], ZSlabDomain.hpp) behind the same
+/// interface; the slabs' initial-condition table is the ts_integrator's.
+template <class Integ, int NC> class SlabAdapter final : public IntegratorIface {
+  public:
+    template <class Model>
+    SlabAdapter(ts_context* ctx, Model&& model, int block_z, double* table, std::size_t table_cap)
+        : dom_(std::forward<Model>(model), amrex::IntVect{1 << 30, 1 << 30, block_z}, ctx), ctx_(ctx), table_(table),
+          table_cap_(table_cap) {}
+    int ncomp() const override { return NC; }
+    void initialise(int kind, int nitems, const double* items) override {
+        if (nitems < 0 || std::size_t(2 + 6 * nitems) > table_cap_) throw std::invalid_argument("too many init items");
+        std::vector<double> host(2 + 6 * std::size_t(nitems));
+        host[0] = kind;
+        host[1] = nitems;
+        for (int q = 0; q < 6 * nitems; ++q) host[2 + q] = items[q];
+        upload(host);
+    }
+    void initialise_expressions(int count, const char* const* exprs) override {
+        if (count != NC) throw std::invalid_argument("one expression per component is required");
+        std::vector<double> host(2 + 2 * NC);
+        host[0] = TS_INIT_EXPRESSION;
+        host[1] = NC;
+        for (int c = 0; c < NC; ++c) {
+            if (!exprs[c]) throw std::invalid_argument("null expression");
+            const std::vector<treesap::expr::Instr> code = treesap::expr::Compiler::compile(exprs[c]);
+            host[2 + c] = double(host.size());
+            host[2 + NC + c] = double(code.size());
+            const std::size_t at = host.size();
+            host.resize(at + 2 * code.size());
+            std::memcpy(host.data() + at, code.data(), sizeof(treesap::expr::Instr) * code.size());
+        }
+        upload(host);
+    }
+    void set_state(const double* src, bool dev) override { dom_.set_state(src, dev); }
+    void get_state(double* dst, bool dev) override { dom_.get_state(dst, dev); }
+    void step() override { dom_.step(); }
+    void step_host_only() override { throw std::invalid_argument("CUDA graphs are not built for z-slab domains"); }
+    double time() const override { return dom_.time(); }
+    long long steps() const override { return dom_.steps(); }
+    void* state_ptr() override { return dom_.slab(0).state().data(); }
+    Layout state_layout() const override { return const_cast<SlabAdapter*>(this)->dom_.slab(0).state().layout(); }
+    long long launches_per_step() const override { return dom_.launches_per_step(); }
+    void attach_clock(treesap::KernelClock* c) override { dom_.attach_clock(c); }
+    void set_launch_shape(int rows, int chunks) override { dom_.set_launch_shape(rows, chunks); }
+    bool state_is_finite() override { return dom_.state_is_finite(); }
+
+  private:
+    void upload(const std::vector<double>& host) {
+        if (host.size() > table_cap_) throw std::invalid_argument("initial condition too long for the parameter table");
+        cudaStream_t s = static_cast<cudaStream_t>(ts_context_stream(ctx_));
+        cuda_check(cudaMemcpyAsync(table_, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice, s),
+                   "cudaMemcpyAsync(init table)");
+        dom_.initialise();
+        cuda_check(cudaStreamSynchronize(s), "cudaStreamSynchronize(initialise)");
+    }
+    treesap::ZSlabDomain<Integ> dom_;
+    ts_context* ctx_;
+    double* table_;
+    std::size_t table_cap_;
+};
+
+/// One z slab of a domain decomposed over processes: the whole-domain Adapter interface on the
+/// slab's own cells (set/get_state take [comp][z_slab][y][x]) plus its stage-level operations.
+template <class Integ, int NC> class RankSlabAdapter final : public IntegratorIface, public SlabOps {
+  public:
+    template <class Model>
+    RankSlabAdapter(ts_context* ctx, Model&& model, const SlabZ& sz, int depth, double* table, std::size_t cap)
+        : inner_(ctx, std::forward<Model>(model), table, cap, sz, depth) {}
+    SlabOps* slab_ops() override { return this; }
+    int ncomp() const override { return NC; }
+    void initialise(int kind, int nitems, const double* items) override { inner_.initialise(kind, nitems, items); }
+    void initialise_expressions(int count, const char* const* exprs) override {
+        inner_.initialise_expressions(count, exprs);
+    }
+    void set_state(const double* src, bool dev) override { inner_.set_state(src, dev); }
+    void get_state(double* dst, bool dev) override { inner_.get_state(dst, dev); }
+    void step() override { throw std::invalid_argument("a slab of a shared domain steps through ts_slab_* calls"); }
+    void step_host_only() override { step(); }
+    double time() const override { return inner_.time(); }
+    long long steps() const override { return inner_.steps(); }
+    void* state_ptr() override { return inner_.state_ptr(); }
+    Layout state_layout() const override { return inner_.state_layout(); }
+    long long launches_per_step() const override { return inner_.launches_per_step(); }
+    void attach_clock(treesap::KernelClock* c) override { inner_.attach_clock(c); }
+    void set_launch_shape(int rows, int chunks) override { inner_.set_launch_shape(rows, chunks); }
+    bool state_is_finite() override { return inner_.state_is_finite(); }
+
+    int stages() const override { return Integ::kStages; }
+    void prepare(int s) override { integ().stage_prepare(s); }
+    void send_planes(int s, int face, void** ptr, long long* elems, long long* cs, int* esize) override {
+        const auto f = integ().stage_ref(s);
+        const Layout& L = f.L;
+        const long long plane = L.px * L.py;
+        const int first = face == 0 ? 0 : L.n[2] - L.g; // its lowest / highest ngrow valid planes
+        *ptr = static_cast<char*>(f.data) + (long long)(first + L.g) * plane * L.esize;
+        *elems = (long long)L.g * plane;
+        *cs = L.comp_stride();
+        *esize = L.esize;
+    }
+    void receive_planes(int s, int face, const void* buf) override {
+        const auto f = integ().stage_ref(s);
+        const Layout& L = f.L;
+        const int kd0 = face == 0 ? -L.g : L.n[2];
+        const long long cs = (long long)L.g * L.px * L.py;
+        if (L.esize == 8)
+            launch_halo_copy(static_cast<double*>(f.data), L, kd0, static_cast<const double*>(buf), cs, L.g,
+                             integ().sm_count(), integ().stream());
+        else
+            launch_halo_copy(static_cast<float*>(f.data), L, kd0, static_cast<const float*>(buf), cs, L.g,
+                             integ().sm_count(), integ().stream());
+    }
+    void fill(int s) override { integ().stage_fill(s, integ().get_model().dt_hint()); }
+    void launch(int s) override { integ().stage_launch(s, integ().get_model().dt_hint()); }
+    void finish() override { integ().stage_finish(integ().get_model().dt_hint()); }
+
+  private:
+    /// The whole-domain adapter's services (table upload, state copies) around the slab integrator.
+    struct Inner {
+        template <class Model>
+        Inner(ts_context* ctx, Model&& model, double* table, std::size_t cap, const SlabZ& sz, int depth)
+            : integ(std::forward<Model>(model), amrex::IntVect{1 << 30, 1 << 30, 1 << 30}, ctx, sz, depth),
+              ctx(ctx), table(table), cap(cap) {}
+        Integ integ;
+        ts_context* ctx;
+        double* table;
+        std::size_t cap;
+        void upload(const std::vector<double>& host) {
+            if (host.size() > cap) throw std::invalid_argument("initial condition too long for the parameter table");
+            cuda_check(cudaMemcpyAsync(table, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                       integ.stream()),
+                       "cudaMemcpyAsync(init table)");
+            integ.initialise();
+            cuda_check(cudaStreamSynchronize(integ.stream()), "cudaStreamSynchronize(initialise)");
+        }
+        void initialise(int kind, int nitems, const double* items) {
+            if (nitems < 0 || std::size_t(2 + 6 * nitems) > cap) throw std::invalid_argument("too many init items");
+            std::vector<double> host(2 + 6 * std::size_t(nitems));
+            host[0] = kind;
+            host[1] = nitems;
+            for (int q = 0; q < 6 * nitems; ++q) host[2 + q] = items[q];
+            upload(host);
+        }
+        void initialise_expressions(int count, const char* const* exprs) {
+            if (count != NC) throw std::invalid_argument("one expression per component is required");
+            std::vector<double> host(2 + 2 * NC);
+            host[0] = TS_INIT_EXPRESSION;
+            host[1] = NC;
+            for (int c = 0; c < NC; ++c) {
+                if (!exprs[c]) throw std::invalid_argument("null expression");
+                const std::vector<treesap::expr::Instr> code = treesap::expr::Compiler::compile(exprs[c]);
+                host[2 + c] = double(host.size());
+                host[2 + NC + c] = double(code.size());
+                const std::size_t at = host.size();
+                host.resize(at + 2 * code.size());
+                std::memcpy(host.data() + at, code.data(), sizeof(treesap::expr::Instr) * code.size());
+            }
+            upload(host);
+        }
+        void set_state(const double* src, bool dev) { integ.set_state(src, dev); }
+        void get_state(double* dst, bool dev) { integ.get_state(dst, dev); }
+        double time() const { return integ.get_time(); }
+        long long steps() const { return (long long)integ.get_steps(); }
+        void* state_ptr() { return integ.state().data(); }
+        Layout state_layout() const { return integ.state().layout(); }
+        long long launches_per_step() const { return integ.launches_per_step(); }
+        void attach_clock(treesap::KernelClock* c) { integ.attach_clock(c); }
+        void set_launch_shape(int rows, int chunks) { integ.set_launch_shape(rows, chunks); }
+        bool state_is_finite() { return integ.state_is_finite(); }
+    };
+    Integ& integ() { return inner_.integ; }
+    Inner inner_;
+};
+
 constexpr std::size_t kInitTableCap = 2 + 6 * 512;
 
 inline amrex::Geometry geometry_of(const ts_wave_desc& d) {
@@ -171,6 +374,37 @@ template <class Model>
 IntegratorIface* make_for_model(ts_context* ctx, const ts_wave_desc& d, Model&& model, double* table) {
     using M = std::decay_t<Model>;
     constexpr int NC = M::ncomp;
+    if (slab_request().active) {
+        const SlabRequest r = slab_request();
+        if (d.precision == TS_PRECISION_F32_STAGE) {
+            if constexpr (treesap::AffineRHSConcept<typename M::rhs_t>) {
+                return new RankSlabAdapter<treesap::SingleLevelRK4F32StageIntegrator<M>, NC>(
+                    ctx, std::forward<Model>(model), r.sz, r.depth, table, kInitTableCap);
+            } else {
+                throw std::invalid_argument("model is not affine: no FP32-stage form");
+            }
+        }
+        if (d.scheme == TS_EULER)
+            return new RankSlabAdapter<treesap::SingleLevelEulerIntegrator<M>, NC>(ctx, std::forward<Model>(model),
+                                                                                r.sz, r.depth, table, kInitTableCap);
+        return new RankSlabAdapter<treesap::SingleLevelRK4Integrator<M>, NC>(ctx, std::forward<Model>(model), r.sz,
+                                                                           r.depth, table, kInitTableCap);
+    }
+    if (d.block[2] > 0 && d.block[2] < d.n[2]) {
+        if (d.precision == TS_PRECISION_F32_STAGE) {
+            if constexpr (treesap::AffineRHSConcept<typename M::rhs_t>) {
+                return new SlabAdapter<treesap::SingleLevelRK4F32StageIntegrator<M>, NC>(
+                    ctx, std::forward<Model>(model), d.block[2], table, kInitTableCap);
+            } else {
+                throw std::invalid_argument("model is not affine: no FP32-stage form");
+            }
+        }
+        if (d.scheme == TS_EULER)
+            return new SlabAdapter<treesap::SingleLevelEulerIntegrator<M>, NC>(ctx, std::forward<Model>(model),
+                                                                            d.block[2], table, kInitTableCap);
+        return new SlabAdapter<treesap::SingleLevelRK4Integrator<M>, NC>(ctx, std::forward<Model>(model), d.block[2],
+                                                                       table, kInitTableCap);
+    }
     if (d.scheme == TS_EULER) {
         if (d.precision != TS_PRECISION_F64) throw std::invalid_argument("Euler runs in FP64 only");
         return new Adapter<treesap::SingleLevelEulerIntegrator<M>, NC>(ctx, std::forward<Model>(model), table,

@@ -50,6 +50,8 @@ ts_status validate(const ts_wave_desc* d) {
         if (!(d->prob_hi[q] > d->prob_lo[q])) return TS_ERR_INVALID_ARGUMENT;
     }
     if (!(d->dt > 0.0)) return TS_ERR_INVALID_ARGUMENT;
+    for (int q = 0; q < 3; ++q)
+        if (d->block[q] < 0) return TS_ERR_INVALID_ARGUMENT;
     if (d->model != TS_MODEL_WAVE && d->model != TS_MODEL_TENSOR_WAVE) return TS_ERR_INVALID_ARGUMENT;
     if (d->scheme != TS_EULER && d->scheme != TS_RK4) return TS_ERR_INVALID_ARGUMENT;
     if (d->precision != TS_PRECISION_F64 && d->precision != TS_PRECISION_F32_STAGE) return TS_ERR_INVALID_ARGUMENT;
@@ -72,6 +74,8 @@ void drop_graphs(ts_integrator* it) {
 }
 
 cudaStream_t stream_of(ts_integrator* it) { return static_cast<cudaStream_t>(ts_context_stream(it->ctx)); }
+
+SlabOps* slab_of(ts_integrator* it) { return it && it->impl ? it->impl->slab_ops() : nullptr; }
 
 } // namespace
 
@@ -116,6 +120,71 @@ ts_status ts_integrator_create(ts_context* ctx, const ts_wave_desc* desc, ts_int
     }
     *out = it;
     return TS_OK;
+}
+
+ts_status ts_integrator_create_slab(ts_context* ctx, const ts_wave_desc* desc, int zlo, int nz, int lo_ex, int hi_ex,
+                                    ts_integrator** out) {
+    if (!ctx || !out || !desc) return TS_ERR_INVALID_ARGUMENT;
+    if (zlo < 0 || nz < desc->ngrow || zlo + nz > desc->n[2] || desc->c2 || desc->model != TS_MODEL_WAVE) {
+        set_error(ctx, "ts_integrator_create_slab: slab outside the domain, thinner than the ghost width, or a model "
+                       "without slab support");
+        return TS_ERR_INVALID_ARGUMENT;
+    }
+    SlabRequest& r = slab_request();
+    r.active = true;
+    r.sz.zoff = zlo;
+    r.sz.nz = desc->n[2];
+    r.sz.lo_ex = lo_ex != 0;
+    r.sz.hi_ex = hi_ex != 0;
+    r.depth = nz;
+    const ts_status st = ts_integrator_create(ctx, desc, out);
+    r = SlabRequest{};
+    return st;
+}
+
+int ts_slab_stages(ts_integrator* it) {
+    SlabOps* s = slab_of(it);
+    return s ? s->stages() : 0;
+}
+
+ts_status ts_slab_prepare(ts_integrator* it, int stage) {
+    SlabOps* s = slab_of(it);
+    if (!s || stage < 0 || stage >= s->stages()) return TS_ERR_INVALID_ARGUMENT;
+    return guarded(it->ctx, "ts_slab_prepare", [&] { s->prepare(stage); });
+}
+
+ts_status ts_slab_send_planes(ts_integrator* it, int stage, int face, void** ptr, long long* elems,
+                              long long* comp_stride, int* elem_size) {
+    SlabOps* s = slab_of(it);
+    if (!s || stage < 0 || stage >= s->stages() || (face != 0 && face != 1) || !ptr || !elems || !comp_stride ||
+        !elem_size)
+        return TS_ERR_INVALID_ARGUMENT;
+    return guarded(it->ctx, "ts_slab_send_planes",
+                   [&] { s->send_planes(stage, face, ptr, elems, comp_stride, elem_size); });
+}
+
+ts_status ts_slab_receive_planes(ts_integrator* it, int stage, int face, const void* buf) {
+    SlabOps* s = slab_of(it);
+    if (!s || stage < 0 || stage >= s->stages() || (face != 0 && face != 1) || !buf) return TS_ERR_INVALID_ARGUMENT;
+    return guarded(it->ctx, "ts_slab_receive_planes", [&] { s->receive_planes(stage, face, buf); });
+}
+
+ts_status ts_slab_fill(ts_integrator* it, int stage) {
+    SlabOps* s = slab_of(it);
+    if (!s || stage < 0 || stage >= s->stages()) return TS_ERR_INVALID_ARGUMENT;
+    return guarded(it->ctx, "ts_slab_fill", [&] { s->fill(stage); });
+}
+
+ts_status ts_slab_launch(ts_integrator* it, int stage) {
+    SlabOps* s = slab_of(it);
+    if (!s || stage < 0 || stage >= s->stages()) return TS_ERR_INVALID_ARGUMENT;
+    return guarded(it->ctx, "ts_slab_launch", [&] { s->launch(stage); });
+}
+
+ts_status ts_slab_finish(ts_integrator* it) {
+    SlabOps* s = slab_of(it);
+    if (!s) return TS_ERR_INVALID_ARGUMENT;
+    return guarded(it->ctx, "ts_slab_finish", [&] { s->finish(); });
 }
 
 ts_status ts_integrator_destroy(ts_integrator* it) {

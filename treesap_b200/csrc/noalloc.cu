@@ -148,7 +148,7 @@ extern "C" ts_status ts_wave_rk4_steps_noalloc(const ts_wave_desc* desc, double*
     if (!desc || !state || nsteps < 0) return TS_ERR_INVALID_ARGUMENT;
     const ts_wave_desc& d = *desc;
     if (d.model != TS_MODEL_WAVE || d.ngrow != 2 || d.scheme != TS_RK4 || d.precision != TS_PRECISION_F64 ||
-        d.abl_thickness > 0 || d.c2 || d.ko_strength < 0.0)
+        d.abl_thickness > 0 || d.c2 || d.ko_strength < 0.0 || (d.block[2] > 0 && d.block[2] < d.n[2]))
         return TS_ERR_UNSUPPORTED;
     for (int q = 0; q < 3; ++q)
         if (d.n[q] < d.ngrow || !(d.prob_hi[q] > d.prob_lo[q])) return TS_ERR_INVALID_ARGUMENT;
