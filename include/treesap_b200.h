@@ -43,7 +43,11 @@ typedef enum ts_status {
 
 typedef enum ts_dtype { TS_F64 = 0, TS_F32 = 1 } ts_dtype;
 typedef enum ts_model { TS_MODEL_WAVE = 0, TS_MODEL_TENSOR_WAVE = 1 } ts_model;
-typedef enum ts_scheme { TS_EULER = 0, TS_RK4 = 1 } ts_scheme;
+typedef enum ts_scheme {
+    TS_EULER = 0,
+    TS_RK4 = 1,
+    TS_DOPRI5 = 2 /* Dormand-Prince 5(4) with step-size control (rtol, atol); FP64, one box */
+} ts_scheme;
 typedef enum ts_bc { TS_BC_NOOP = 0, TS_BC_DIRICHLET = 1 } ts_bc;
 typedef enum ts_precision {
     TS_PRECISION_F64 = 0,      /* plain form: FP64 throughout, the reference's register scheme */
@@ -145,6 +149,7 @@ typedef struct ts_wave_desc {
                               * planes are exchanged every stage; the result is bitwise the single box's.
                               * block[0], block[1] (and 0 = the whole domain) keep one box in x and y, which
                               * the stage kernels tile themselves. */
+    double rtol, atol;       /* TS_DOPRI5: relative / absolute error tolerance (0: 1e-6 / 1e-9) */
 } ts_wave_desc;
 
 typedef struct ts_integrator ts_integrator;
@@ -226,6 +231,12 @@ TS_API ts_status ts_integrator_state_field(ts_integrator* it, void** device_ptr,
 /* Capture one step into a CUDA graph and replay it for subsequent ts_integrator_step calls
  * (enable != 0), or go back to per-kernel launches (enable == 0). */
 TS_API ts_status ts_integrator_use_graph(ts_integrator* it, int enable);
+/* TS_DOPRI5 integrators: steps accepted and rejected since the last initialise / set_state, the
+ * step size proposed for the next step and the scaled error norm of the last attempt. Each
+ * ts_integrator_step call advances one accepted step (retrying rejected ones); the simulation
+ * time (ts_integrator_time) is the sum of the accepted step sizes. */
+TS_API ts_status ts_integrator_adaptive_stats(ts_integrator* it, long long* accepted, long long* rejected,
+                                              double* next_dt, double* last_error);
 /* Health check (no counterpart in the reference): waits for the integrator's stream and scans
  * the valid cells of the state; TS_ERR_NONFINITE when any value is NaN or infinite. */
 TS_API ts_status ts_integrator_check_finite(ts_integrator* it);

@@ -25,6 +25,7 @@ __all__ = [
     "Adjoint",
     "TS_EULER",
     "TS_RK4",
+    "TS_DOPRI5",
     "TS_F64",
     "TS_F32_STAGE",
     "TS_BC_NOOP",
@@ -41,7 +42,7 @@ __all__ = [
 LIB_PATH = Path(__file__).resolve().with_name("libtreesap_b200.so")
 
 TS_OK = 0
-TS_EULER, TS_RK4 = 0, 1
+TS_EULER, TS_RK4, TS_DOPRI5 = 0, 1, 2
 TS_F64, TS_F32_STAGE = 0, 1
 TS_BC_NOOP, TS_BC_DIRICHLET = 0, 1
 TS_INIT_STATE, TS_INIT_GAUSSIAN, TS_INIT_FOURIER, TS_INIT_EXPRESSION = 0, 1, 2, 3
@@ -86,6 +87,8 @@ class WaveDesc(C.Structure):
         ("precision", C.c_int),
         ("c2", C.c_void_p),
         ("block", C.c_int * 3),
+        ("rtol", C.c_double),
+        ("atol", C.c_double),
     ]
 
     def ncomp(self) -> int:
@@ -151,6 +154,7 @@ def lib() -> C.CDLL:
         "ts_integrator_state_field": (i, [vp, C.POINTER(vp), C.POINTER(FieldLayout)]),
         "ts_integrator_use_graph": (i, [vp, i]),
         "ts_integrator_check_finite": (i, [vp]),
+        "ts_integrator_adaptive_stats": (i, [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(d), C.POINTER(d)]),
         "ts_integrator_create_slab": (i, [vp, C.POINTER(WaveDesc), i, i, i, i, C.POINTER(vp)]),
         "ts_slab_stages": (i, [vp]),
         "ts_slab_prepare": (i, [vp, i]),
@@ -291,6 +295,13 @@ class Integrator:
             "ts_integrator_run",
             self.ctx,
         )
+
+    def adaptive_stats(self) -> dict:
+        """TS_DOPRI5: accepted / rejected steps, the next proposed dt and the last error norm."""
+        a, r, dt, e = C.c_longlong(), C.c_longlong(), C.c_double(), C.c_double()
+        _check(lib().ts_integrator_adaptive_stats(self.handle, C.byref(a), C.byref(r), C.byref(dt), C.byref(e)),
+               "ts_integrator_adaptive_stats", self.ctx)
+        return {"accepted": a.value, "rejected": r.value, "next_dt": dt.value, "last_error": e.value}
 
     def check_finite(self) -> None:
         """Raises TSError(TS_ERR_NONFINITE) when the state holds NaN or infinite values."""

@@ -39,6 +39,8 @@ def wave_desc(
     prob_hi=(1.0, 1.0, 1.0),
     model: int = TS_MODEL_WAVE,
     block=(0, 0, 0),
+    rtol: float = 0.0,
+    atol: float = 0.0,
 ) -> WaveDesc:
     d = WaveDesc()
     n = (n, n, n) if np.isscalar(n) else tuple(n)
@@ -61,6 +63,8 @@ def wave_desc(
     d.precision = precision
     d.c2 = None
     d.block[:] = list(block)
+    d.rtol = rtol
+    d.atol = atol
     return d
 
 

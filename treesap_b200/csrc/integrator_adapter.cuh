@@ -12,6 +12,7 @@
 
 #include <treesap_b200.h>
 
+#include "integrators/SingleLevelDOPRI5Integrator.hpp"
 #include "integrators/SingleLevelEulerIntegrator.hpp"
 #include "integrators/SingleLevelRK4F32StageIntegrator.hpp"
 #include "integrators/SingleLevelRK4Integrator.hpp"
@@ -110,6 +111,9 @@ struct IntegratorIface {
     virtual void attach_clock(treesap::KernelClock* c) = 0;
     virtual void set_launch_shape(int rows, int chunks) = 0;
     virtual bool state_is_finite() = 0;
+    virtual void adaptive_stats(long long*, long long*, double*, double*) {
+        throw std::invalid_argument("not an adaptive (TS_DOPRI5) integrator");
+    }
 };
 
 /// Exposes the protected time / step counters of the front-end integrators.
@@ -124,10 +128,20 @@ template <class Integ> struct Exposed : Integ {
 
 template <class Integ, int NC> class Adapter final : public IntegratorIface {
   public:
-    template <class Model>
-    Adapter(ts_context* ctx, Model&& model, double* table, std::size_t table_cap)
-        : integ_(std::forward<Model>(model), amrex::IntVect{1 << 30, 1 << 30, 1 << 30}, ctx), table_(table),
+    template <class Model, class... Extra>
+    Adapter(ts_context* ctx, Model&& model, double* table, std::size_t table_cap, Extra... extra)
+        : integ_(std::forward<Model>(model), amrex::IntVect{1 << 30, 1 << 30, 1 << 30}, ctx, extra...), table_(table),
           table_cap_(table_cap) {}
+    void adaptive_stats(long long* acc, long long* rej, double* next_dt, double* err) override {
+        if constexpr (requires { integ_.accepted(); }) {
+            *acc = integ_.accepted();
+            *rej = integ_.rejected();
+            *next_dt = integ_.proposed_dt();
+            *err = integ_.last_error();
+        } else {
+            IntegratorIface::adaptive_stats(acc, rej, next_dt, err);
+        }
+    }
     int ncomp() const override { return NC; }
     void initialise(int kind, int nitems, const double* items) override {
         if (nitems < 0 || std::size_t(2 + 6 * nitems) > table_cap_) throw std::invalid_argument("too many init items");
@@ -389,6 +403,13 @@ IntegratorIface* make_for_model(ts_context* ctx, const ts_wave_desc& d, Model&& 
                                                                                 r.sz, r.depth, table, kInitTableCap);
         return new RankSlabAdapter<treesap::SingleLevelRK4Integrator<M>, NC>(ctx, std::forward<Model>(model), r.sz,
                                                                            r.depth, table, kInitTableCap);
+    }
+    if (d.scheme == TS_DOPRI5) {
+        if (d.precision != TS_PRECISION_F64 || (d.block[2] > 0 && d.block[2] < d.n[2]))
+            throw std::invalid_argument("DOPRI5 runs in FP64 on one box");
+        return new Adapter<treesap::SingleLevelDOPRI5Integrator<M>, NC>(ctx, std::forward<Model>(model), table,
+                                                                         kInitTableCap, d.rtol > 0.0 ? d.rtol : 1e-6,
+                                                                         d.atol > 0.0 ? d.atol : 1e-9);
     }
     if (d.block[2] > 0 && d.block[2] < d.n[2]) {
         if (d.precision == TS_PRECISION_F32_STAGE) {

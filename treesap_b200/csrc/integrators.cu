@@ -53,7 +53,8 @@ ts_status validate(const ts_wave_desc* d) {
     for (int q = 0; q < 3; ++q)
         if (d->block[q] < 0) return TS_ERR_INVALID_ARGUMENT;
     if (d->model != TS_MODEL_WAVE && d->model != TS_MODEL_TENSOR_WAVE) return TS_ERR_INVALID_ARGUMENT;
-    if (d->scheme != TS_EULER && d->scheme != TS_RK4) return TS_ERR_INVALID_ARGUMENT;
+    if (d->scheme != TS_EULER && d->scheme != TS_RK4 && d->scheme != TS_DOPRI5) return TS_ERR_INVALID_ARGUMENT;
+    if (d->rtol < 0.0 || d->atol < 0.0) return TS_ERR_INVALID_ARGUMENT;
     if (d->precision != TS_PRECISION_F64 && d->precision != TS_PRECISION_F32_STAGE) return TS_ERR_INVALID_ARGUMENT;
     if (d->precision == TS_PRECISION_F32_STAGE && d->scheme != TS_RK4) return TS_ERR_UNSUPPORTED;
     if (d->abl_thickness < 0 || (d->abl_thickness > 0 && d->abl_profile != 1 && d->abl_profile != 2))
@@ -235,6 +236,13 @@ ts_status ts_integrator_set_state(ts_integrator* it, const double* src, int src_
 ts_status ts_integrator_get_state(ts_integrator* it, double* dst, int dst_is_device) {
     if (!it || !it->impl || !dst) return TS_ERR_INVALID_ARGUMENT;
     return guarded(it->ctx, "ts_integrator_get_state", [&] { it->impl->get_state(dst, dst_is_device != 0); });
+}
+
+ts_status ts_integrator_adaptive_stats(ts_integrator* it, long long* accepted, long long* rejected, double* next_dt,
+                                       double* last_error) {
+    if (!it || !it->impl || !accepted || !rejected || !next_dt || !last_error) return TS_ERR_INVALID_ARGUMENT;
+    return guarded(it->ctx, "ts_integrator_adaptive_stats",
+                   [&] { it->impl->adaptive_stats(accepted, rejected, next_dt, last_error); });
 }
 
 ts_status ts_integrator_check_finite(ts_integrator* it) {
