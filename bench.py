@@ -72,9 +72,13 @@ class Dist:
             import torch
             import torch.distributed as dist
 
-            # host tensors (barriers, timings) over gloo, device tensors (slab planes) over NCCL
-            torch.cuda.set_device(local_rank)
-            dist.init_process_group("cpu:gloo,cuda:nccl", timeout=datetime.timedelta(seconds=300))
+            # host tensors (barriers, timings) over gloo, device tensors (slab planes) over NCCL;
+            # gloo alone on a host without a GPU (the host-side logic runs there too)
+            backend = "gloo"
+            if torch.cuda.is_available():
+                torch.cuda.set_device(local_rank)
+                backend = "cpu:gloo,cuda:nccl"
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
             self.dist = dist
 
     def barrier(self):
