@@ -469,7 +469,10 @@ def run_b200(args, rank, world, local_rank):
                    "fd_directions": a["directions"], "fd_rel_err_max_phi0": a["fd_rel_max_phi0"],
                    "fd_rel_err_max_c": a["fd_rel_max_c"], "tolerance": 1e-5,
                    "fp32_stage": {"state_gradient_seconds": a["fp32_stage_state_gradient_s"],
+                                  "gradient_seconds": a["fp32_stage_gradient_s"],
                                   "grad_phi0_maxnorm_rel_vs_fp64": a["fp32_stage_grad_phi0_rel_vs_fp64"],
+                                  "grad_c_maxnorm_rel_vs_fp64": a["fp32_stage_grad_c_rel_vs_fp64"],
+                                  "fd_rel_err_max_c": a["fp32_stage_fd_rel_max_c"],
                                   "loss_rel_vs_fp64": a["fp32_stage_loss_rel_vs_fp64"]}}
     except Exception as ex:  # noqa: BLE001 - reported in the line
         adjoint = {"error": str(ex)}

@@ -307,11 +307,14 @@ TS_API ts_status ts_adjoint_forward(ts_adjoint* a, const double* phi0, const dou
 TS_API ts_status ts_adjoint_gradient(ts_adjoint* a, const double* phi0, const double* pi0, const double* c, int nsteps,
                                      const double* phi_target, double* loss, double* grad_phi0, double* grad_pi0,
                                      double* grad_c);
-/* FP32-stage form of J and dJ/dphi0, dJ/dpi0: forward run and reverse sweep in the FP32-stage
- * RK4 form (FP32 stage arithmetic and storage, FP64 states); the speed gradient is FP64 only. */
+/* FP32-stage form of J and dJ/dphi0, dJ/dpi0, dJ/dc: forward run and reverse sweep in the
+ * FP32-stage RK4 form (stencils of the stage differences in FP32, FP64 states). The state
+ * gradient needs no checkpoints; the speed gradient (grad_c non-NULL) recomputes each forward
+ * step's FP32-stage registers from checkpoints taken every `checkpoint_every` steps, like
+ * ts_adjoint_gradient. Any output may be NULL. */
 TS_API ts_status ts_adjoint_gradient_f32(ts_adjoint* a, const double* phi0, const double* pi0, const double* c,
                                          int nsteps, const double* phi_target, double* loss, double* grad_phi0,
-                                         double* grad_pi0);
+                                         double* grad_pi0, double* grad_c);
 /* Tangent-linear run: the perturbation (dphi(T), dpi(T)) caused by (dphi0, dpi0, dc) (NULL = 0). */
 TS_API ts_status ts_adjoint_tangent(ts_adjoint* a, const double* phi0, const double* pi0, const double* c,
                                     const double* dphi0, const double* dpi0, const double* dc, int nsteps,

@@ -112,15 +112,32 @@ def test_fp32_stage_state_gradient_vs_fp64(ctx, ngrow):
     d, c, phi0, pi0, target = setup(24, ngrow)
     adj = Adjoint(ctx, d, 5)
     l64, g64, p64, _ = adj.gradient(phi0, pi0, c, 20, target)
-    l32, g32, p32 = adj.gradient_f32(phi0, pi0, c, 20, target)
+    l32, g32, p32, c32 = adj.gradient_f32(phi0, pi0, c, 20, target, speed=False)
+    assert c32 is None
     assert abs(l32 - l64) <= 1e-6 * abs(l64)
     assert relmax(g32, g64) <= 1e-6 and relmax(p32, p64) <= 1e-6
+
+
+@pytest.mark.parametrize("ngrow,every,nsteps", [(2, 5, 20), (4, 7, 17), (2, 30, 13), (2, 1, 6)])
+def test_fp32_stage_speed_gradient_vs_fp64(ctx, ngrow, every, nsteps):
+    """FP32-stage speed gradient (forward and adjoint registers of each step recomputed from
+    checkpoints) within 1e-6 of the FP64 speed gradient, for checkpoint intervals that divide
+    the run, that do not, that exceed it and of one step; the state gradient is the one of the
+    state-only call, bitwise."""
+    d, c, phi0, pi0, target = setup(24, ngrow)
+    adj = Adjoint(ctx, d, every)
+    l64, g64, p64, c64 = adj.gradient(phi0, pi0, c, nsteps, target)
+    l32, g32, p32, c32 = adj.gradient_f32(phi0, pi0, c, nsteps, target)
+    _, g32s, p32s, _ = adj.gradient_f32(phi0, pi0, c, nsteps, target, speed=False)
+    assert abs(l32 - l64) <= 1e-6 * abs(l64)
+    assert relmax(c32, c64) <= 1e-6, relmax(c32, c64)
+    assert np.array_equal(g32, g32s) and np.array_equal(p32, p32s)
 
 
 def test_fp32_stage_state_gradient_matches_central_differences(ctx):
     d, c, phi0, pi0, target = setup(20, 2)
     adj = Adjoint(ctx, d, 5)
-    _, g32, _ = adj.gradient_f32(phi0, pi0, c, 12, target)
+    _, g32, _, _ = adj.gradient_f32(phi0, pi0, c, 12, target, speed=False)
     rng = np.random.default_rng(5)
     for _ in range(3):
         v = rng.standard_normal(phi0.shape)
@@ -129,8 +146,30 @@ def test_fp32_stage_state_gradient_matches_central_differences(ctx):
         # error at any step; a wide step keeps the FP32-stage rounding of J (about 1e-8 of J)
         # small against the difference itself.
         eps = 0.1
-        lp = adj.gradient_f32(phi0 + eps * v, pi0, c, 12, target)[0]
-        lm = adj.gradient_f32(phi0 - eps * v, pi0, c, 12, target)[0]
+        lp = adj.gradient_f32(phi0 + eps * v, pi0, c, 12, target, speed=False)[0]
+        lm = adj.gradient_f32(phi0 - eps * v, pi0, c, 12, target, speed=False)[0]
         fd = (lp - lm) / (2 * eps)
         ad = float(np.sum(g32 * v))
+        assert abs(fd - ad) <= 1e-5 * abs(ad), (fd, ad)
+
+
+def test_fp32_stage_speed_gradient_matches_central_differences(ctx):
+    """<dJ/dc, v> of the FP32-stage form against central differences of the FP64 loss (the
+    FP32-stage loss rounds at about 1e-8 of J, too coarse for a difference quotient in c)."""
+    d, c, phi0, pi0, target = setup(24, 2)
+    nsteps = 20
+    adj = Adjoint(ctx, d, 6)
+    _, _, _, gc = adj.gradient_f32(phi0, pi0, c, nsteps, target)
+    rng = np.random.default_rng(12)
+
+    def loss(c_):
+        phiT, _ = adj.forward(phi0, pi0, c_, nsteps)
+        return 0.5 * float(np.sum((phiT - target) ** 2))
+
+    for _ in range(3):
+        v = rng.standard_normal(c.shape)
+        v /= np.linalg.norm(v)
+        eps = 1e-5
+        fd = (loss(c + eps * v) - loss(c - eps * v)) / (2 * eps)
+        ad = float(np.sum(gc * v))
         assert abs(fd - ad) <= 1e-5 * abs(ad), (fd, ad)

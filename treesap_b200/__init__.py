@@ -7,6 +7,7 @@ loudly when the library has not been built.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import weakref
 from pathlib import Path
@@ -184,7 +185,7 @@ def lib() -> C.CDLL:
         "ts_adjoint_forward": (i, [vp, vp, vp, vp, i, vp, vp]),
         "ts_adjoint_gradient": (i, [vp, vp, vp, vp, i, vp, C.POINTER(d), vp, vp, vp]),
         "ts_adjoint_tangent": (i, [vp, vp, vp, vp, vp, vp, vp, i, vp, vp]),
-        "ts_adjoint_gradient_f32": (i, [vp, vp, vp, vp, i, vp, C.POINTER(d), vp, vp]),
+        "ts_adjoint_gradient_f32": (i, [vp, vp, vp, vp, i, vp, C.POINTER(d), vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -202,6 +203,21 @@ def _check(status: int, what: str, ctx: "Context | None" = None) -> None:
         raise TSError(status, what, detail)
 
 
+_live_contexts: weakref.WeakSet = weakref.WeakSet()
+
+
+@atexit.register
+def _close_live_contexts() -> None:
+    """Closes every context still open when the interpreter exits, each after its integrators,
+    batches and adjoints, while the interpreter and the library are still intact (module
+    teardown would otherwise destroy handles in no defined order)."""
+    for ctx in list(_live_contexts):
+        try:
+            ctx.close()
+        except Exception:
+            pass
+
+
 class Context:
     """One device, one CUDA stream (ts_context)."""
 
@@ -209,6 +225,7 @@ class Context:
         self.handle = C.c_void_p()
         self._dependents = weakref.WeakSet()  # integrators / batches, destroyed before the context
         _check(lib().ts_context_create(device, C.byref(self.handle)), "ts_context_create")
+        _live_contexts.add(self)
 
     def _adopt(self, obj) -> None:
         self._dependents.add(obj)
@@ -452,15 +469,17 @@ class Adjoint:
                "ts_adjoint_gradient", self.ctx)
         return loss.value, gphi, gpi, gc
 
-    def gradient_f32(self, phi0, pi0, c, nsteps: int, target):
-        """FP32-stage form: (J, dJ/dphi0, dJ/dpi0)."""
+    def gradient_f32(self, phi0, pi0, c, nsteps: int, target, speed: bool = True):
+        """FP32-stage form: (J, dJ/dphi0, dJ/dpi0, dJ/dc); dJ/dc is None when speed is False
+        (the state gradient alone needs no checkpoints)."""
         phi0, pi0, c, target = self._in(phi0), self._in(pi0), self._in(c), self._in(target)
         gphi, gpi = np.empty(self.shape), np.empty(self.shape)
+        gc = np.empty(self.shape) if speed else None
         loss = C.c_double()
         _check(lib().ts_adjoint_gradient_f32(self.handle, _ptr(phi0), _ptr(pi0), _ptr(c), nsteps, _ptr(target),
-                                             C.byref(loss), _ptr(gphi), _ptr(gpi)),
+                                             C.byref(loss), _ptr(gphi), _ptr(gpi), _ptr(gc)),
                "ts_adjoint_gradient_f32", self.ctx)
-        return loss.value, gphi, gpi
+        return loss.value, gphi, gpi, gc
 
     def tangent(self, phi0, pi0, c, dphi0, dpi0, dc, nsteps: int):
         args = [self._in(a) for a in (phi0, pi0, c, dphi0, dpi0, dc)]

@@ -131,6 +131,24 @@ template <int ngrow_> struct WaveC2LaplacianRHS {
     }
 };
 
+/// {D phi, 0} of a two-component field {phi, pi} (or of its FP32-stage registers k0, d1, d2):
+/// the Laplacian behind the FP32-stage form of the speed gradient.
+template <int ngrow_> struct WaveLaplacianRHS {
+    static constexpr int ncomp = 2;
+    static constexpr int ngrow = ngrow_;
+    struct Workspace {};
+
+    template <int comp, typename T>
+    AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE T operator()(const amrex::IntVect idx, amrex::Real,
+                                                          const amrex::Array4<const T>& arr,
+                                                          const amrex::GeometryData& geom, Workspace&) const {
+        if constexpr (comp == 0)
+            return detail::lap<ngrow>(arr, 0, idx, geom);
+        else
+            return T(0);
+    }
+};
+
 /// Adjoint model {phibar, pibar} with the speed as a coefficient field instead of a state
 /// component: phibar_t = s K phibar + D (c2 pibar), pibar_t = phibar + s K pibar, c2 read from a
 /// device array of the valid cells (x fastest) with periodic wrap-around at the neighbour taps.

@@ -53,9 +53,129 @@ struct EpiSpeedGradient {
     }
 };
 
+/// The FP32-stage form of the speed-gradient accumulation, term Q of one step:
+///   g += coef_Q * D X_Q,   X_Q = u, k0 (FP64 stencils), d1, d2 (FP32 stencils),
+/// where u, k0, d1, d2 are the forward step's FP32-stage registers and the forward stage
+/// arguments are w0 = u, w1 = u + dt/2 k0, w2 = u + dt/2 (k0 + d1), w3 = u + dt (k0 + d2).
+/// With A_s the pi component of the adjoint stage argument s (from the adjoint step's
+/// registers lam, kb0, db1, db2: A0 = lam, A1 = lam + dt/2 kb0, A2 = lam + dt/2 (kb0 + db1),
+/// A3 = lam + dt (kb0 + db2)) and beta_s = dt b_s, the step's term sum_s beta_s A_s D w_{3-s}
+/// regroups into
+///   coef_u = sum_s beta_s A_s,  coef_k0 = dt (beta_0 A0 + beta_1 A1 / 2 + beta_2 A2 / 2),
+///   coef_d1 = dt / 2 beta_1 A1, coef_d2 = dt beta_0 A0.
+/// The adjoint registers and g are read at the cell from global memory.
+struct SpeedGradF32Params {
+    double* g;
+    Layout Lg;
+    const double* lam;
+    const double* kb0;
+    Layout Lu;
+    const float* db1;
+    const float* db2;
+    Layout Lf;
+    double dt;
+};
+template <int Q> struct EpiSpeedGradF32 : NoCentre {
+    using Params = SpeedGradF32Params;
+    template <class T, int NC, int CX, class CO>
+    static __device__ __forceinline__ void apply(const Params& p, const T (&k)[CX][NC], const bool (&act)[CX],
+                                                 const T*, int, int i0, int j, int z, const CO&) {
+#pragma unroll
+        for (int e = 0; e < CX; ++e) {
+            if (!act[e]) continue;
+            const long long ou = p.Lu.index(i0 + e, j, z, 1);
+            const long long of = p.Lf.index(i0 + e, j, z, 1);
+            const double lam = p.lam[ou], kb = p.kb0[ou];
+            const double dt = p.dt, b0 = dt / 6.0, b1 = dt / 3.0;
+            double coef;
+            if constexpr (Q == 0) {
+                const double a1 = lam + 0.5 * dt * kb, a2 = lam + 0.5 * dt * (kb + double(p.db1[of]));
+                const double a3 = lam + dt * (kb + double(p.db2[of]));
+                coef = b0 * lam + b1 * a1 + b1 * a2 + b0 * a3;
+            } else if constexpr (Q == 1) {
+                const double a1 = lam + 0.5 * dt * kb, a2 = lam + 0.5 * dt * (kb + double(p.db1[of]));
+                coef = dt * (b0 * lam + 0.5 * b1 * a1 + 0.5 * b1 * a2);
+            } else if constexpr (Q == 2) {
+                coef = 0.5 * dt * b1 * (lam + 0.5 * dt * kb);
+            } else {
+                coef = dt * b0 * lam;
+            }
+            double* g = p.g + p.Lg.index(i0 + e, j, z, 0);
+            *g += coef * double(k[e][0]);
+        }
+    }
+};
+
 } // namespace treesap_b200
 
 namespace treesap {
+
+/// Launches the four FP32-stage speed-gradient terms of one step (EpiSpeedGradF32) on the
+/// registers of a forward and an adjoint FP32-stage RK4 step of the two-component wave system.
+template <int G> class WaveSpeedGradientF32 {
+  public:
+    using Lap = tsb::WaveLaplacianRHS<G>;
+    using Tile64 = typename detail::DefaultTile<double, G, 2>::type;
+    using Tile32 = typename detail::DefaultTile<float, G, 2>::type;
+    struct Reg {
+        void* data;
+        treesap_b200::Layout L;
+    };
+
+    WaveSpeedGradientF32(ts_context* ctx_, const amrex::GeometryData& geom_) : ctx(ctx_), geom(geom_) {}
+
+    /// g += the step's speed-gradient term (g: one FP64 component, any layout of the domain).
+    /// fwd, adj: the registers u, k0, d1, d2 of the forward and of the adjoint step.
+    void accumulate(const Reg (&fwd)[4], const Reg (&adj)[4], double* g, const treesap_b200::Layout& Lg, double dt) {
+        using namespace treesap_b200;
+        const auto make = [&]() {
+            SpeedGradF32Params p{};
+            p.g = g;
+            p.Lg = Lg;
+            p.lam = static_cast<const double*>(adj[0].data);
+            p.kb0 = static_cast<const double*>(adj[1].data);
+            p.Lu = adj[0].L;
+            p.db1 = static_cast<const float*>(adj[2].data);
+            p.db2 = static_cast<const float*>(adj[3].data);
+            p.Lf = adj[2].L;
+            p.dt = dt;
+            return p;
+        };
+        const auto p = make();
+        term<0, double, Tile64>(fwd[0], p);
+        term<1, double, Tile64>(fwd[1], p);
+        term<2, float, Tile32>(fwd[2], p);
+        term<3, float, Tile32>(fwd[3], p);
+    }
+
+  private:
+    template <int Q, class T, class Cfg> void term(const Reg& in, const treesap_b200::SpeedGradF32Params& ep) {
+        using namespace treesap_b200;
+        using Epi = EpiSpeedGradF32<Q>;
+        using Launcher = StageLauncher<Cfg, Lap, Epi>;
+        const Layout& L = in.L;
+        const int sm = ts_context_sm_count(ctx);
+        const auto shape = Launcher::shape(L, sm);
+        const CUtensorMap& tm = tmaps.get(in.data, L, sizeof(T) == 8 ? TS_F64 : TS_F32, Launcher::box_x(),
+                                          Launcher::box_y(shape));
+        const CentreMaps cm = Launcher::centre_maps(
+            [this](const void* b, const Layout& Lc, int dtype, int bx, int by) -> const CUtensorMap& {
+                return tmaps.get(b, Lc, dtype, bx, by);
+            },
+            ep, shape);
+        StageParams<T> sp{};
+        sp.in = static_cast<const T*>(in.data);
+        sp.L = L;
+        sp.geom = geom;
+        sp.time = 0.0;
+        sp.err = ts_context_error_word(ctx);
+        Launcher::launch(tm, cm, sp, Lap{}, ep, shape, static_cast<cudaStream_t>(ts_context_stream(ctx)));
+    }
+
+    ts_context* ctx;
+    amrex::GeometryData geom;
+    treesap_b200::TensorMapCache tmaps;
+};
 
 template <int G> class WaveAdjointRK4 {
   public:

@@ -83,10 +83,11 @@ ts_status ts_adjoint_gradient(ts_adjoint* a, const double* phi0, const double* p
 }
 
 ts_status ts_adjoint_gradient_f32(ts_adjoint* a, const double* phi0, const double* pi0, const double* c, int nsteps,
-                                  const double* phi_target, double* loss, double* grad_phi0, double* grad_pi0) {
+                                  const double* phi_target, double* loss, double* grad_phi0, double* grad_pi0,
+                                  double* grad_c) {
     if (!a || !a->impl || !phi0 || !c || !phi_target || nsteps < 1) return TS_ERR_INVALID_ARGUMENT;
     return guarded(a->ctx, "ts_adjoint_gradient_f32", [&] {
-        const double l = a->impl->state_gradient_f32(phi0, pi0, c, nsteps, phi_target, grad_phi0, grad_pi0);
+        const double l = a->impl->gradient_f32(phi0, pi0, c, nsteps, phi_target, grad_phi0, grad_pi0, grad_c);
         if (loss) *loss = l;
     });
 }

@@ -92,9 +92,21 @@ inline SlabRequest& slab_request() {
     return r;
 }
 
+/// Stage-level stepping of a whole-domain RK4-family integrator with access to its stage
+/// registers: after run_stage(s), field(s) is the input of stage s with its ghost cells filled
+/// (FP32-stage form: u, k0, d1, d2), valid until finish() ends the step.
+struct StageOps {
+    virtual ~StageOps() = default;
+    virtual int stages() const = 0;
+    virtual void run_stage(int s) = 0;
+    virtual void finish() = 0;
+    virtual void field(int s, void** data, Layout* L) = 0;
+};
+
 struct IntegratorIface {
     virtual ~IntegratorIface() = default;
     virtual SlabOps* slab_ops() { return nullptr; }
+    virtual StageOps* stage_ops() { return nullptr; }
     virtual int ncomp() const = 0;
     virtual void initialise(int kind, int nitems, const double* items) = 0;
     /// Expression initial condition: one expression of x, y, z per component.
@@ -126,12 +138,40 @@ template <class Integ> struct Exposed : Integ {
     }
 };
 
-template <class Integ, int NC> class Adapter final : public IntegratorIface {
+template <class Integ, int NC> class Adapter final : public IntegratorIface, public StageOps {
+    static constexpr bool kStageApi = requires(Integ& i) { i.stage_launch(0, 0.0); };
+
   public:
     template <class Model, class... Extra>
     Adapter(ts_context* ctx, Model&& model, double* table, std::size_t table_cap, Extra... extra)
         : integ_(std::forward<Model>(model), amrex::IntVect{1 << 30, 1 << 30, 1 << 30}, ctx, extra...), table_(table),
           table_cap_(table_cap) {}
+    StageOps* stage_ops() override {
+        if constexpr (kStageApi) return this;
+        return nullptr;
+    }
+    int stages() const override {
+        if constexpr (kStageApi) return Integ::kStages;
+        return 0;
+    }
+    void run_stage(int s) override {
+        if constexpr (kStageApi) {
+            const double dt = integ_.get_model().dt_hint();
+            integ_.stage_prepare(s);
+            integ_.stage_fill(s, dt);
+            integ_.stage_launch(s, dt);
+        }
+    }
+    void finish() override {
+        if constexpr (kStageApi) integ_.stage_finish(integ_.get_model().dt_hint());
+    }
+    void field(int s, void** data, Layout* L) override {
+        if constexpr (kStageApi) {
+            const auto f = integ_.stage_ref(s);
+            *data = f.data;
+            *L = f.L;
+        }
+    }
     void adaptive_stats(long long* acc, long long* rej, double* next_dt, double* err) override {
         if constexpr (requires { integ_.accepted(); }) {
             *acc = integ_.accepted();

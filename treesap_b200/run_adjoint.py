@@ -7,7 +7,9 @@
 phi_target from a forward run of the pulse shifted by 2 cells and scaled by 1.05. Prints the
 time of one loss+gradient evaluation and, per random unit direction v of phi0 and of c, the
 relative difference between <grad, v> and (J(p + eps v) - J(p - eps v)) / (2 eps); then the
-FP32-stage form of the initial-state gradient (time, and its difference to the FP64 one).
+FP32-stage form: the time of J + state gradient and of J + state and speed gradients, their
+max-norm differences to the FP64 gradients, and the speed gradient against the same central
+differences (of the FP64 loss).
 """
 from __future__ import annotations
 
@@ -39,8 +41,17 @@ def run(ctx, n=128, steps=C5_STEPS, every=C5_CHECKPOINT_EVERY, directions=32, se
         phiT, _ = adj.forward(p, pi0, c_, steps)
         return 0.5 * float(np.sum((phiT - target) ** 2))
 
+    # FP32-stage form: state gradient alone, then state and speed gradients
+    adj.gradient_f32(phi0, pi0, c, steps, target, speed=False)  # warm-up
+    t0 = time.perf_counter()
+    adj.gradient_f32(phi0, pi0, c, steps, target, speed=False)
+    t_state32 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    loss32, gphi32, _, gc32 = adj.gradient_f32(phi0, pi0, c, steps, target)
+    t_grad32 = time.perf_counter() - t0
+
     rng = np.random.default_rng(seed)
-    rel = {"phi0": [], "c": []}
+    rel = {"phi0": [], "c": [], "c32": []}
     for _ in range(directions):
         v = rng.standard_normal(phi0.shape)
         v /= np.linalg.norm(v)
@@ -49,19 +60,22 @@ def run(ctx, n=128, steps=C5_STEPS, every=C5_CHECKPOINT_EVERY, directions=32, se
                 fd = (J(phi0 + eps * v, c) - J(phi0 - eps * v, c)) / (2 * eps)
             else:
                 fd = (J(phi0, c + eps * v) - J(phi0, c - eps * v)) / (2 * eps)
+                ad32 = float(np.sum(gc32 * v))
+                rel["c32"].append(abs(fd - ad32) / abs(ad32))
             ad = float(np.sum(g * v))
             rel[name].append(abs(fd - ad) / abs(ad))
-    # FP32-stage form of the initial-state gradient
-    adj.gradient_f32(phi0, pi0, c, steps, target)  # warm-up
-    t0 = time.perf_counter()
-    loss32, gphi32, _ = adj.gradient_f32(phi0, pi0, c, steps, target)
-    t_grad32 = time.perf_counter() - t0
-    rel32 = float(np.abs(gphi32 - gphi).max() / np.abs(gphi).max())
     adj.close()
+
+    def relmax(a, b):
+        return float(np.abs(a - b).max() / np.abs(b).max())
+
     return {"loss": loss, "cells": n**3, "steps": steps, "checkpoint_every": every, "gradient_s": t_grad,
             "forward_s": t_fwd, "fd_rel_max_phi0": max(rel["phi0"]), "fd_rel_max_c": max(rel["c"]),
-            "directions": directions, "fp32_stage_state_gradient_s": t_grad32,
-            "fp32_stage_grad_phi0_rel_vs_fp64": rel32,
+            "directions": directions, "fp32_stage_state_gradient_s": t_state32,
+            "fp32_stage_gradient_s": t_grad32,
+            "fp32_stage_grad_phi0_rel_vs_fp64": relmax(gphi32, gphi),
+            "fp32_stage_grad_c_rel_vs_fp64": relmax(gc32, gc),
+            "fp32_stage_fd_rel_max_c": max(rel["c32"]),
             "fp32_stage_loss_rel_vs_fp64": abs(loss32 - loss) / abs(loss)}
 
 

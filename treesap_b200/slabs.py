@@ -60,6 +60,7 @@ class GpuSlab:
                                          C.byref(self.handle))
         if st != 0:
             raise TSError(st, "ts_integrator_create_slab", (L.ts_context_last_error(ctx.handle) or b"").decode())
+        ctx._adopt(self)  # destroyed before the context
         self.ncomp = desc.ncomp()
         self.shape = (self.ncomp, nz, desc.n[1], desc.n[0])
         self.stages = L.ts_slab_stages(self.handle)
