@@ -25,8 +25,11 @@ struct Layout {
     long long px = 0, py = 0, pz = 0;
 
     AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE long long comp_stride() const { return px * py * pz; }
+    /// Row (k, j) of a component as a 32-bit number (make() guarantees py pz < 2^31), widened once
+    /// by the row pitch: one 32x32->64 multiply per index instead of 64-bit products.
     AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE long long index(int i, int j, int k, int c) const {
-        return c * comp_stride() + (long long)(k + g) * px * py + (long long)(j + g) * px + (i + xoff);
+        const int row = (k + g) * int(py) + (j + g);
+        return c * comp_stride() + (long long)row * int(px) + (i + xoff);
     }
     AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE long long elements() const { return comp_stride() * nc; }
     long long bytes() const { return elements() * esize; }
@@ -44,7 +47,14 @@ struct Layout {
         L.px = round_up(L.xoff + n_[0] + g_, a);
         L.py = n_[1] + 2 * g_;
         L.pz = n_[2] + 2 * g_;
+        if (!rows_fit(n_, g_)) throw std::invalid_argument("field extents beyond 2^31 rows per component");
         return L;
+    }
+    /// Whether index() can count the rows (y-z) of one component and the row pitch in 32 bits.
+    static bool rows_fit(const int n_[3], int g_) {
+        const long long py_ = (long long)n_[1] + 2 * g_, pz_ = (long long)n_[2] + 2 * g_;
+        const long long px_ = (long long)n_[0] + 4 * g_ + 8;
+        return py_ * pz_ < (1LL << 31) && px_ < (1LL << 31);
     }
     ts_field_layout to_c(int dtype) const {
         ts_field_layout c{};

@@ -179,6 +179,7 @@ ts_status ts_field_layout_make(const int n[3], int ngrow, int ncomp, int dtype, 
         return TS_ERR_INVALID_ARGUMENT;
     for (int d = 0; d < 3; ++d)
         if (n[d] < 1 || n[d] < ngrow) return TS_ERR_INVALID_ARGUMENT;
+    if (!Layout::rows_fit(n, ngrow)) return TS_ERR_INVALID_ARGUMENT;
     const Layout L = Layout::make(n, ngrow, ncomp, dtype == TS_F64 ? 8 : 4);
     *out = L.to_c(dtype);
     return TS_OK;
