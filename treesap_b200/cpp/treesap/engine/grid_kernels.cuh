@@ -114,7 +114,14 @@ __device__ __forceinline__ void ghost_fill_cell(T* __restrict__ f, const Layout&
     int s[3] = {i, j, k + sz.zoff};
     bool inside = true;
     for (int d = 0; d < 3; ++d) {
-        if (geom.is_periodic[d]) s[d] = ((s[d] % n[d]) + n[d]) % n[d];
+        // a ghost coordinate lies within one period of the domain when ngrow <= n, so the
+        // periodic image is one conditional shift (an integer modulo by a run-time n costs
+        // dozens of instructions, and this runs for every ghost cell of every fill); smaller
+        // domains take more shifts
+        if (geom.is_periodic[d]) {
+            while (s[d] < 0) s[d] += n[d];
+            while (s[d] >= n[d]) s[d] -= n[d];
+        }
         if (s[d] < 0 || s[d] >= n[d]) inside = false;
     }
     const long long cs = L.comp_stride();
@@ -198,29 +205,30 @@ void launch_ghost_fill(T* f, const Layout& L, const amrex::GeometryData& geom, c
 /// src[c * src_cs + p * px * py + (j + g) * px + i + xoff] (src: a neighbour field from its
 /// plane ks0 on, or a staging buffer of whole planes received from another GPU).
 template <class T>
-__global__ void halo_copy_kernel(T* __restrict__ dst, const Layout Ld, int kd0, const T* __restrict__ src,
-                                 long long src_cs, int np) {
-    const long long row = Ld.n[0], rows = Ld.n[1], plane = Ld.px * Ld.py;
-    const long long total = (long long)Ld.nc * np * rows * row;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int i = int(t % row);
-        long long r = t / row;
-        const int j = int(r % rows);
-        r /= rows;
-        const int p = int(r % np), c = int(r / np);
-        dst[Ld.index(i, j, kd0 + p, c)] = src[c * src_cs + p * plane + (long long)(j + Ld.g) * Ld.px + i + Ld.xoff];
+__global__ void __launch_bounds__(128) halo_copy_kernel(T* __restrict__ dst, const Layout Ld, int kd0,
+                                                        const T* __restrict__ src, long long src_cs, int np) {
+    // one row (c, p, j) per block iteration, its cells over the threads: the per-row index split
+    // is block-uniform, so no thread divides
+    const int rows = Ld.n[1];
+    const long long nrows = (long long)Ld.nc * np * rows, plane = Ld.px * Ld.py;
+    for (long long q = blockIdx.x; q < nrows; q += gridDim.x) {
+        const int j = int(q % rows);
+        const long long cp = q / rows;
+        const int p = int(cp % np), c = int(cp / np);
+        T* d = dst + Ld.index(0, j, kd0 + p, c);
+        const T* s = src + c * src_cs + p * plane + (long long)(j + Ld.g) * Ld.px + Ld.xoff;
+        for (int i = threadIdx.x; i < Ld.n[0]; i += blockDim.x) d[i] = s[i];
     }
 }
 
 template <class T>
 void launch_halo_copy(T* dst, const Layout& Ld, int kd0, const T* src, long long src_cs, int np, int sm_count,
                       cudaStream_t stream) {
-    const long long total = (long long)Ld.nc * np * Ld.n[1] * Ld.n[0];
-    if (total == 0) return;
-    long long blocks = (total + 255) / 256;
-    if (blocks > (long long)sm_count * 16) blocks = (long long)sm_count * 16;
-    halo_copy_kernel<T><<<int(blocks), 256, 0, stream>>>(dst, Ld, kd0, src, src_cs, np);
+    const long long nrows = (long long)Ld.nc * np * Ld.n[1];
+    if (nrows == 0 || Ld.n[0] == 0) return;
+    long long blocks = nrows;
+    if (blocks > (long long)sm_count * 32) blocks = (long long)sm_count * 32;
+    halo_copy_kernel<T><<<int(blocks), 128, 0, stream>>>(dst, Ld, kd0, src, src_cs, np);
     cuda_check(cudaGetLastError(), "halo_copy_kernel launch");
 }
 

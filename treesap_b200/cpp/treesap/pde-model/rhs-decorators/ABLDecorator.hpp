@@ -63,9 +63,9 @@ struct ABLDecorator {
             ws.have_sigma = true;
         }
         const T inner = T(rhs.template operator()<comp>(idx, time, arr, geom, ws.inner));
-        // Inside the bulk sigma is 0 and the damping term vanishes: skip it (for finite states
-        // F - 0 (u - target) is F; whole warps of bulk cells take this branch together).
-        if (ws.sigma_value == 0.0) return inner;
+        // No branch on sigma == 0 here (inside the bulk the term is F - 0 (u - target) = F):
+        // measured, the branch per component costs more than the two operations it skips.
+        // sigma() itself returns early in the bulk, which skips the square root.
         return inner - T(ws.sigma_value) * (arr(idx, comp) - T(data.target_values[comp]));
     }
 
