@@ -59,6 +59,9 @@ def test_invalid_arguments_are_rejected():
     L = tsb.FieldLayout()
     assert lib.ts_field_layout_make((C.c_int * 3)(3, 3, 3), 4, 2, 0, C.byref(L)) == 1  # n < ngrow
     assert lib.ts_field_layout_make((C.c_int * 3)(8, 8, 8), 2, 0, 0, C.byref(L)) == 1  # ncomp 0
+    # the stage kernels count the rows of a component (y x z with ghosts) in 32 bits
+    assert lib.ts_field_layout_make((C.c_int * 3)(64, 46340, 46340), 2, 1, 0, C.byref(L)) == 1
+    assert lib.ts_field_layout_make((C.c_int * 3)(64, 46000, 46000), 2, 1, 0, C.byref(L)) == 0
     assert lib.ts_integrator_create(None, None, None) == 1
     assert lib.ts_context_sync(None) == 1
 
