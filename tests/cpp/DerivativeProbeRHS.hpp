@@ -6,7 +6,8 @@
 //   d_t u = D_x v + D_y v + a D_xxx u + b D_xyz u
 //   d_t v = D_z u + c D_xxy v + c D_yz u
 // The coefficients only need to keep a few steps bounded; the system is not meant to be a
-// physical model.
+// physical model. It is linear and autonomous and templated on the value type of the array, so
+// it also runs in the FP32-stage RK4 form (against the reference headers T is double).
 #pragma once
 
 #include "pde-model/PDEModelConcepts.hpp"
@@ -17,27 +18,29 @@ template <int ngrow_> struct DerivativeProbeRHS {
     static constexpr int ncomp = 2;
     static constexpr int ngrow = ngrow_;
     static_assert(ngrow >= 2, "third derivatives need ngrow >= 2");
+    static constexpr bool is_affine_autonomous = true;
 
     struct Workspace {};
 
     amrex::Real a = 1e-4, b = 2e-4, c = 1e-4;
 
-    template <int comp>
-    AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE amrex::Real operator()(const amrex::IntVect idx, amrex::Real,
-                                                                    const amrex::Array4<const amrex::Real>& arr,
-                                                                    const amrex::GeometryData& geom, Workspace&) const {
+    template <int comp, typename T>
+    AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE T operator()(const amrex::IntVect idx, amrex::Real,
+                                                          const amrex::Array4<const T>& arr,
+                                                          const amrex::GeometryData& geom, Workspace&) const {
         using namespace treesap;
         using namespace treesap::tensor;
         using namespace treesap::stencil;
-        ScalarAlias<0> u{{arr}};
-        ScalarAlias<u.next> v{{arr}};
+        ScalarAlias<0, const T> u{{arr}};
+        ScalarAlias<u.next, const T> v{{arr}};
         static_assert(v.next == ncomp);
         if constexpr (u.contains(comp)) {
             return derivative<ngrow, 0>(v, {}, idx, geom) + derivative<ngrow, 1>(v, {}, idx, geom) +
-                   a * derivative<ngrow, 0, 0, 0>(u, {}, idx, geom) + b * derivative<ngrow, 0, 1, 2>(u, {}, idx, geom);
+                   T(a) * derivative<ngrow, 0, 0, 0>(u, {}, idx, geom) +
+                   T(b) * derivative<ngrow, 0, 1, 2>(u, {}, idx, geom);
         } else {
-            return derivative<ngrow, 2>(u, {}, idx, geom) + c * derivative<ngrow, 0, 0, 1>(v, {}, idx, geom) +
-                   c * derivative<ngrow, 1, 2>(u, {}, idx, geom);
+            return derivative<ngrow, 2>(u, {}, idx, geom) + T(c) * derivative<ngrow, 0, 0, 1>(v, {}, idx, geom) +
+                   T(c) * derivative<ngrow, 1, 2>(u, {}, idx, geom);
         }
     }
 };

@@ -6,6 +6,7 @@
 #include <AMReX.H>
 
 #include "integrators/SingleLevelEulerIntegrator.hpp"
+#include "integrators/SingleLevelRK4F32StageIntegrator.hpp"
 #include "integrators/SingleLevelRK4Integrator.hpp"
 
 #include "examples_run.hpp"
@@ -13,6 +14,10 @@
 
 #include <exception>
 #include <cstdio>
+
+/// Integrator code of the front end's FP32-stage RK4 form (GPU side only; the reference has
+/// no such form, so its results are compared with the reference's FP64 RK4).
+constexpr int kRK4F32Stage = 2;
 
 #ifdef TSB_EX_G
 // One translation unit per stencil half-width (TSB_EX_G = 1..4), compiled in parallel.
@@ -33,6 +38,13 @@ extern "C" int TSB_EX_CAT(tsb_example_run_g, TSB_EX_G)(int example, const tsref_
             if (d->integrator == TSREF_RK4) {
                 treesap::SingleLevelRK4Integrator<M> integ(std::move(model), block);
                 go(integ);
+            } else if (d->integrator == kRK4F32Stage) {
+                if constexpr (treesap::AffineRHSConcept<typename M::rhs_t>) {
+                    treesap::SingleLevelRK4F32StageIntegrator<M> integ(std::move(model), block);
+                    go(integ);
+                } else {
+                    throw std::invalid_argument("the FP32-stage form needs an affine model");
+                }
             } else {
                 treesap::SingleLevelEulerIntegrator<M> integ(std::move(model), block);
                 go(integ);

@@ -11,7 +11,9 @@ relative max-norm (the plain form's bar) for every ngrow 1..4, with and without 
 Dirichlet and periodic boundaries, RK4 and Euler, one box and several (block_size).
 
 The same holds for DerivativeProbeRHS (tests/cpp), a test-only model that runs the first- and
-third-derivative stencils, unmixed and mixed, that the built-in models never use.
+third-derivative stencils, unmixed and mixed, that the built-in models never use. Being linear,
+the probe also runs in the FP32-stage RK4 form, checked against the reference's FP64 RK4 at
+1e-6.
 """
 import numpy as np
 import pytest
@@ -101,3 +103,20 @@ def test_nonlinear_example_is_nonlinear(sides):
     a = gpu.run(2, d, s0, 4, 0.0)
     b = gpu.run(2, d, s0, 4, 0.5)
     assert relerr(a, b) > 1e-8
+
+
+@pytest.mark.parametrize("ngrow,periodic,ko", [(2, (0, 0, 0), 0.0), (3, (1, 1, 1), 0.1), (4, (0, 1, 0), 0.05)])
+def test_derivative_probe_in_the_fp32_stage_form(sides, ngrow, periodic, ko):
+    """The D1/D3 probe (linear, value-type generic) in the FP32-stage RK4 form: its FP32
+    stencils of the stage differences stay within 1e-6 of the reference's FP64 RK4."""
+    ref, gpu = sides
+    n = (29, 23, 19)
+    d = desc(n, ngrow, periodic=periodic, ko=ko, bc=1, bc_values=(0.05, 0.0), integrator=1)
+    s0 = initial_state(3, n, seed=300 + ngrow)
+    want = ref.run(3, d, s0, 6, 0.0)
+    d.integrator = 2  # the front end's FP32-stage RK4
+    got = gpu.run(3, d, s0, 6, 0.0)
+    assert np.isfinite(got).all()
+    err = relerr(got, want)
+    assert err <= 1e-6, err
+    assert err > 0.0  # the FP32 stages did run (FP64 would agree to ~1e-15)
