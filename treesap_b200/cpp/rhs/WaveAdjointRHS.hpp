@@ -22,8 +22,9 @@
 namespace tsb {
 
 namespace detail {
-/// base + s sum_a KO_a of component n, the KODecorator's arithmetic (its one-pass form), or
-/// base when s = 0.
+/// base + s sum_a KO_a of component n in the one-pass form, which is KODecorator's
+/// arithmetic for models of at most 4 components (so the 3-component forward model is bitwise
+/// the 2-component library model), or base when s = 0.
 template <int G, typename T>
 AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE T with_ko(T base, const amrex::Array4<const T>& arr, int n,
                                                    const amrex::IntVect& idx, const amrex::GeometryData& geom,
