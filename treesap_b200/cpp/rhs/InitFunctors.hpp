@@ -59,6 +59,9 @@ template <int ncomp_> struct FourierSumInit {
 /// (ABLProfileConcept, reference pde-model/rhs-decorators/ABLDecorator.hpp:24-29).
 struct QuadraticProfile {
     constexpr amrex::Real operator()(amrex::Real s) const { return s * s; }
+    /// The same profile as a function of s^2 (the B200 front end's ABLDecorator then needs no
+    /// square root and no branch; the reference calls operator() only).
+    constexpr amrex::Real of_square(amrex::Real s2) const { return s2; }
 };
 struct LinearProfile {
     constexpr amrex::Real operator()(amrex::Real s) const { return s; }
