@@ -126,3 +126,15 @@ def test_bounds_checked_view_flags_out_of_range_reads(tmp_path):
     assert r["in_plane"] == 34 and r["in_glob"] == 1000 + (8 * 35 + 4 * 5 + 3) and r["err_in"] == 0
     assert r["err_plane"] == 2 and r["out_plane"] == 17
     assert r["err_glob"] == 2 and r["out_glob"] == 1000 + 4 * 35 + 17
+
+
+def test_quadratic_layer_sigma_matches_the_square_root_path(tmp_path):
+    """The branch-free damping strength of a profile with of_square (QuadraticProfile) equals the
+    reference's path (square root of the squared index distance, then the profile) to rounding
+    at every cell of the layer, and is exactly 0 in the bulk."""
+    exe = tmp_path / "abl_sigma"
+    subprocess.run(["g++", "-std=c++20", "-O1", *INC, str(ROOT / "tests/cpp/abl_sigma_probe.cpp"), "-o", str(exe)],
+                   check=True)
+    r = json.loads(subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout)
+    assert r["bulk_zero"] and r["layer_cells"] == 64**3 - 32**3
+    assert r["worst_rel"] <= 4e-16
