@@ -11,8 +11,8 @@
  *
  * HBM layout of a field (all state and stage buffers): component-major, [comp][z][y][x] with
  * x fastest, `ngrow` ghost cells on every face, the x origin shifted by `xoff` (ngrow rounded
- * up to 16 bytes) so that interior rows start 16-byte aligned, and the row pitch padded to
- * 16 bytes:  element (i, j, k, c) is at  ((c*pz + k+ngrow)*py + j+ngrow)*px + i+xoff
+ * up to 32 bytes) so that interior rows start on a 32-byte sector, and the row pitch padded to
+ * 32 bytes:  element (i, j, k, c) is at  ((c*pz + k+ngrow)*py + j+ngrow)*px + i+xoff
  * for i in [-ngrow, n0+ngrow), j in [-ngrow, n1+ngrow), k in [-ngrow, n2+ngrow).
  */
 #ifndef TREESAP_B200_H
@@ -102,7 +102,7 @@ typedef struct ts_field_layout {
     int ngrow;         /* ghost width */
     int ncomp;
     int dtype;         /* ts_dtype */
-    int xoff;          /* x index of cell i = 0 within a row, ngrow rounded up to 16 bytes */
+    int xoff;          /* x index of cell i = 0 within a row, ngrow rounded up to 32 bytes */
     int reserved;
     long long px, py, pz; /* padded extents (elements): row pitch, rows per plane, planes per component */
 } ts_field_layout;

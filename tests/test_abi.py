@@ -47,9 +47,9 @@ def test_field_layout_rules(dtype, esize, ngrow):
     n = (C.c_int * 3)(37, 29, 41)
     L = tsb.FieldLayout()
     assert lib.ts_field_layout_make(n, ngrow, 2, dtype, C.byref(L)) == 0
-    a = 16 // esize
-    assert L.xoff == -(-ngrow // a) * a  # ngrow rounded up to 16 bytes
-    assert (L.xoff * esize) % 16 == 0 and (L.px * esize) % 16 == 0  # TMA stride / alignment rules
+    a = 32 // esize
+    assert L.xoff == -(-ngrow // a) * a  # ngrow rounded up to a 32-byte sector
+    assert (L.xoff * esize) % 32 == 0 and (L.px * esize) % 32 == 0  # whole sectors; TMA needs 16 bytes
     assert L.px >= L.xoff + 37 + ngrow and L.py == 29 + 2 * ngrow and L.pz == 41 + 2 * ngrow
     assert lib.ts_field_bytes(C.byref(L)) == L.px * L.py * L.pz * 2 * esize
 

@@ -42,7 +42,10 @@ struct Layout {
         L.g = g_;
         L.nc = nc_;
         L.esize = esize_;
-        const int a = 16 / esize_;
+        // x origin and row pitch on 32-byte sector boundaries: rows of valid cells then start and
+        // end on whole sectors wherever the extent allows, so stores of whole rows leave no
+        // partly written sector for the memory to read back
+        const int a = 32 / esize_;
         L.xoff = round_up(g_, a);
         L.px = round_up(L.xoff + n_[0] + g_, a);
         L.py = n_[1] + 2 * g_;

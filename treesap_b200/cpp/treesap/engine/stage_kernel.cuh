@@ -379,6 +379,7 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
             for (int m = 0; m < nitems && ok; ++m) {
                 const ItemBox b = src.item(m);
                 const int skip = src.params(b.inst).skip_plane;
+                const int xs = src.params(b.inst).L.xoff - XH; // storage x of the box start minus x0
                 wl = src.params(b.inst).wait_ns;
                 const CUtensorMap* tmap = src.stencil_map(b.inst);
                 const CentreMaps& cm = src.centre_maps(b.inst);
@@ -416,8 +417,10 @@ template <class Cfg, class RHS, class Epi, class Src> __device__ __forceinline__
                         continue;
                     }
                     ptx::mbar_arrive_expect_tx(&full[ps.s], bytes + (centre ? cbytes : 0u));
-                    // storage coordinates: x = x0 - XH + xoff (= x0), y = y0 - G + g (= y0), z = z0 - G + q + g
-                    ptx::tma_load_4d(smem_raw + ps.s * SSLOT, tmap, b.x0, b.y0, b.z0 + q + (G - ZH), 0, &full[ps.s]);
+                    // storage coordinates: x = x0 - XH + xoff, y = y0 - G + g (= y0), z = z0 - G + q + g;
+                    // xoff - XH is 0 or 16 bytes (xoff: ngrow rounded up to 32 bytes, XH: to 16)
+                    ptx::tma_load_4d(smem_raw + ps.s * SSLOT, tmap, b.x0 + xs, b.y0, b.z0 + q + (G - ZH), 0,
+                                     &full[ps.s]);
                     if constexpr (NCEN > 0) {
                         if (centre) {
                             const int zc = b.z0 - 2 * ZH + q;
