@@ -1,7 +1,7 @@
 // treesap-b200 engine: ghost fill, initialisation and host-order pack/unpack kernels.
 //
-// Ghost fill (the single-level FillPatch of SingleLevelIntegrator.hpp:153-163): one thread
-// per ghost cell, all components. A ghost cell whose coordinates, wrapped in the periodic
+// Ghost fill (the single-level FillPatch of SingleLevelIntegrator.hpp:153-163): each thread
+// fills a few ghost cells, all components. A ghost cell whose coordinates, wrapped in the periodic
 // directions, land inside the domain takes that valid cell's value; every other ghost cell
 // (outside the domain grown by the ghost width in periodic directions only) is handed to
 // the model's BC functor (DirichletBC.hpp:43-65 writes its values to all components,
@@ -14,6 +14,8 @@
 
 #include <AMReX.H>
 #include <cuda_runtime.h>
+
+#include <type_traits>
 
 #include "../util/static_for.hpp"
 #include "field.hpp"
@@ -98,17 +100,24 @@ AMREX_GPU_HOST_DEVICE inline void ghost_coords(const Layout& L, long long t, int
     i = ii < g ? ii - g : n0 + (ii - g);
 }
 
-/// Fills ghost cell number t of field f (slab enumeration of ghost_coords).
+/// What the fill does with one ghost cell: its storage offset, and for a periodic image the
+/// offset of the valid cell it copies.
+struct GhostTarget {
+    enum Kind : int { Skip = 0, Copy = 1, Zero = 2, Functor = 3 };
+    long long dst, src;
+    int kind;
+};
+
+/// Resolves ghost cell number t of a field (slab enumeration of ghost_coords).
 /// For a z slab (sz.nz > 0) the ghost cells of exchange planes (sz.lo_ex / sz.hi_ex) are left to
 /// the halo exchange, and the domain tests and the BC functor use global z (local + sz.zoff);
-/// the periodic source of every other ghost cell lies in the slab's own planes.
-template <class T, class BC>
-__device__ __forceinline__ void ghost_fill_cell(T* __restrict__ f, const Layout& L, const amrex::GeometryData& geom,
-                                                const BC& bc, const amrex::BCRec* bcr, double time, int mode,
-                                                long long t, const SlabZ& sz = SlabZ{}) {
+/// the periodic source of every other ghost cell lies in the slab's own planes, so a source is
+/// always a valid cell and never another ghost cell of the same fill.
+__device__ __forceinline__ GhostTarget ghost_target(const Layout& L, const amrex::GeometryData& geom, int mode,
+                                                    long long t, const SlabZ& sz) {
     int i, j, k;
     ghost_coords(L, t, i, j, k);
-    if ((k < 0 && sz.lo_ex) || (k >= L.n[2] && sz.hi_ex)) return; // filled by the halo exchange
+    if ((k < 0 && sz.lo_ex) || (k >= L.n[2] && sz.hi_ex)) return {0, 0, GhostTarget::Skip};
     const int nzg = sz.nz > 0 ? sz.nz : L.n[2];
     const int n[3] = {L.n[0], L.n[1], nzg};
     int s[3] = {i, j, k + sz.zoff};
@@ -124,28 +133,63 @@ __device__ __forceinline__ void ghost_fill_cell(T* __restrict__ f, const Layout&
         }
         if (s[d] < 0 || s[d] >= n[d]) inside = false;
     }
+    const long long dst = L.index(i, j, k, 0);
+    if (inside) return {dst, L.index(s[0], s[1], s[2] - sz.zoff, 0), GhostTarget::Copy};
+    if (mode == int(GhostMode::Homogeneous)) return {dst, 0, GhostTarget::Zero};
+    if (mode == int(GhostMode::Functor)) return {dst, 0, GhostTarget::Functor};
+    return {0, 0, GhostTarget::Skip};
+}
+
+/// Fills ghost cells t0, t0 + step, ..., t0 + (K-1) step (those below `end`) of field f.
+/// The K cells are resolved first and each component's K source values are loaded before any
+/// is stored, so a thread keeps K loads in flight: one load-store pair at a time leaves too
+/// few bytes in flight per SM to cover the DRAM latency, and the fill then runs at about
+/// half the HBM bandwidth.
+template <int K, class T, class BC>
+__device__ __forceinline__ void ghost_fill_cells(T* __restrict__ f, const Layout& L, const amrex::GeometryData& geom,
+                                                 const BC& bc, const amrex::BCRec* bcr, double time, int mode,
+                                                 long long t0, long long step, long long end,
+                                                 const SlabZ& sz = SlabZ{}) {
+    GhostTarget tg[K];
+    unsigned functor_cells = 0;
+#pragma unroll
+    for (int u = 0; u < K; ++u) {
+        const long long t = t0 + u * step;
+        tg[u] = t < end ? ghost_target(L, geom, mode, t, sz) : GhostTarget{0, 0, GhostTarget::Skip};
+        if (tg[u].kind == GhostTarget::Functor) functor_cells |= 1u << u;
+    }
     const long long cs = L.comp_stride();
-    if (inside) {
-        const long long dst = L.index(i, j, k, 0), src = L.index(s[0], s[1], s[2] - sz.zoff, 0);
-        for (int c = 0; c < L.nc; ++c) f[dst + c * cs] = f[src + c * cs];
-    } else if (mode == int(GhostMode::Homogeneous)) {
-        const long long dst = L.index(i, j, k, 0);
-        for (int c = 0; c < L.nc; ++c) f[dst + c * cs] = T(0);
-    } else if (mode == int(GhostMode::Functor)) {
-        if constexpr (std::is_same_v<T, amrex::Real>) {
+    for (int c = 0; c < L.nc; ++c) {
+        T v[K];
+#pragma unroll
+        for (int u = 0; u < K; ++u) v[u] = tg[u].kind == GhostTarget::Copy ? f[tg[u].src + c * cs] : T(0);
+#pragma unroll
+        for (int u = 0; u < K; ++u)
+            if (tg[u].kind == GhostTarget::Copy || tg[u].kind == GhostTarget::Zero) f[tg[u].dst + c * cs] = v[u];
+    }
+    if constexpr (std::is_same_v<T, amrex::Real>) {
+        // cells outside the domain (non-periodic faces) go to the model's BC functor one by one
+        while (functor_cells) {
+            const int u = __ffs(int(functor_cells)) - 1;
+            functor_cells &= functor_cells - 1;
+            int i, j, k;
+            ghost_coords(L, t0 + u * step, i, j, k);
             const amrex::Array4<amrex::Real> dest = make_array4(f, L, sz.zoff);
             bc(amrex::IntVect{i, j, k + sz.zoff}, dest, 0, L.nc, geom, time, bcr, 0, 0);
         }
     }
 }
 
+/// Ghost cells per thread and pass of the single-field fill.
+constexpr int kGhostUnroll = 4;
+
 template <class T, class BC>
 __global__ void ghost_fill_kernel(T* __restrict__ f, const Layout L, const amrex::GeometryData geom, const BC bc,
                                   const amrex::BCRec* bcr, double time, int mode, const SlabZ sz) {
     const long long total = ghost_count(L).total();
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x)
-        ghost_fill_cell(f, L, geom, bc, bcr, time, mode, t, sz);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += kGhostUnroll * stride)
+        ghost_fill_cells<kGhostUnroll>(f, L, geom, bc, bcr, time, mode, t, stride, total, sz);
 }
 
 /// One field of a batched ghost fill.
@@ -166,23 +210,36 @@ struct GhostChunk {
 };
 constexpr int kGhostChunk = 2048;
 
+/// Threads of a batched ghost-fill block; each fills kGhostUnroll cells of a chunk per pass.
+constexpr int kGhostFillThreads = 256;
+
 /// Ghost fill of many fields in one launch: block b fills the ghost cells of chunk b (its
-/// entry read once per block from global memory into shared memory).
+/// entry read once per block from global memory into shared memory). At least 4 blocks per SM
+/// (64 registers a thread): 1024 threads per SM, each with kGhostUnroll loads in flight.
 template <class T, class BC>
-__global__ void __launch_bounds__(256) batch_ghost_fill_kernel(const GhostEntry<T, BC>* __restrict__ entries,
-                                                              const GhostChunk* __restrict__ chunks, int nchunks,
-                                                              const amrex::BCRec* bcr) {
-    __shared__ __align__(16) unsigned char raw[sizeof(GhostEntry<T, BC>)];
-    auto& e = *reinterpret_cast<GhostEntry<T, BC>*>(raw);
+__global__ void __launch_bounds__(kGhostFillThreads, 4) batch_ghost_fill_kernel(const GhostEntry<T, BC>* __restrict__ entries,
+                                                                            const GhostChunk* __restrict__ chunks,
+                                                                            int nchunks, const amrex::BCRec* bcr) {
+    using E = GhostEntry<T, BC>;
+    constexpr int K = kGhostUnroll;
+    __shared__ __align__(16) unsigned char raw[sizeof(E)];
+    auto& e = *reinterpret_cast<E*>(raw);
     for (int b = blockIdx.x; b < nchunks; b += gridDim.x) {
         const GhostChunk ch = chunks[b];
         __syncthreads(); // the previous chunk's threads are done with the entry
-        if (threadIdx.x == 0) e = entries[ch.entry];
+        if constexpr (std::is_trivially_copyable_v<E> && sizeof(E) % 8 == 0 && alignof(E) >= 8) {
+            // one 8-byte word per thread: a single memory round trip instead of thread 0's serial copy
+            const auto* q = reinterpret_cast<const unsigned long long*>(entries + ch.entry);
+            auto* r = reinterpret_cast<unsigned long long*>(raw);
+            for (int w = threadIdx.x; w < int(sizeof(E) / 8); w += blockDim.x) r[w] = q[w];
+        } else {
+            if (threadIdx.x == 0) e = entries[ch.entry];
+        }
         __syncthreads();
         const long long total = ghost_count(e.L).total();
         const long long end = ch.first + kGhostChunk < total ? ch.first + kGhostChunk : total;
-        for (long long t = ch.first + threadIdx.x; t < end; t += blockDim.x)
-            ghost_fill_cell(e.f, e.L, e.geom, e.bc, bcr, e.time, e.mode, t);
+        for (long long t = ch.first + threadIdx.x; t < end; t += (long long)K * blockDim.x)
+            ghost_fill_cells<K>(e.f, e.L, e.geom, e.bc, bcr, e.time, e.mode, t, blockDim.x, end);
     }
 }
 

@@ -378,7 +378,7 @@ class BatchedRK4Integrator {
             if (chunks.n == 0) return;
             int blocks = chunks.n;
             if (blocks > 32 * sms) blocks = 32 * sms;
-            treesap_b200::batch_ghost_fill_kernel<T, BCType><<<blocks, 256, 0, s>>>(entries.p, chunks.p, chunks.n, bcr);
+            treesap_b200::batch_ghost_fill_kernel<T, BCType><<<blocks, treesap_b200::kGhostFillThreads, 0, s>>>(entries.p, chunks.p, chunks.n, bcr);
             treesap_b200::cuda_check(cudaGetLastError(), "batch_ghost_fill_kernel launch");
         }
     };
