@@ -27,7 +27,7 @@ VARIANTS = {
     "two FP64 cells per thread, short prefetch": ["-DTREESAP_B200_TILE_F64=204221", "-DTREESAP_B200_TILE_F32=103221"],
     "z taps from global memory": ["-DTREESAP_B200_QUEUE_MAX_COMPONENTS=0"],
     # bounds-checked build: every shared-memory and global stencil access is range-checked and an
-    # out-of-range index would set the device error word (the driver then exits non-zero)
+    # out-of-range index would set the device error word (the test program then exits non-zero)
     "bounds-checked": ["-DTREESAP_B200_CHECK=1"],
     "bounds-checked, z taps from global memory": ["-DTREESAP_B200_CHECK=1", "-DTREESAP_B200_QUEUE_MAX_COMPONENTS=0"],
 }
