@@ -210,18 +210,21 @@ struct GhostChunk {
 };
 constexpr int kGhostChunk = 2048;
 
-/// Threads of a batched ghost-fill block; each fills kGhostUnroll cells of a chunk per pass.
+/// Threads of a batched ghost-fill block, and the ghost cells each fills per pass: 3 cells
+/// fit the 64 registers of 4 blocks per SM without spills (4 cells spilled into local memory,
+/// whose traffic nearly matched the fill's own loads).
 constexpr int kGhostFillThreads = 256;
+constexpr int kBatchGhostUnroll = 3;
 
 /// Ghost fill of many fields in one launch: block b fills the ghost cells of chunk b (its
 /// entry read once per block from global memory into shared memory). At least 4 blocks per SM
-/// (64 registers a thread): 1024 threads per SM, each with kGhostUnroll loads in flight.
+/// (64 registers a thread): 1024 threads per SM, each with kBatchGhostUnroll loads in flight.
 template <class T, class BC>
 __global__ void __launch_bounds__(kGhostFillThreads, 4) batch_ghost_fill_kernel(const GhostEntry<T, BC>* __restrict__ entries,
                                                                             const GhostChunk* __restrict__ chunks,
                                                                             int nchunks, const amrex::BCRec* bcr) {
     using E = GhostEntry<T, BC>;
-    constexpr int K = kGhostUnroll;
+    constexpr int K = kBatchGhostUnroll;
     __shared__ __align__(16) unsigned char raw[sizeof(E)];
     auto& e = *reinterpret_cast<E*>(raw);
     for (int b = blockIdx.x; b < nchunks; b += gridDim.x) {
