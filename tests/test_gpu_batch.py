@@ -64,6 +64,30 @@ def test_batch_matches_single_box_bitwise(ctx, precision, ngrow, ko, periodic):
         assert np.array_equal(got, want), (i, relerr(got, want))
 
 
+@pytest.mark.parametrize("precision", [TS_F64, TS_F32_STAGE])
+def test_batch_mixed_periodicity_matches_single_box_bitwise(ctx, precision):
+    """Instances periodic in different directions (Dirichlet data on their other faces) in one
+    batch: the batched ghost fill resolves periodic images and boundary cells per instance, and
+    a thread's cells mix both kinds at the edges and corners of the faces."""
+    shapes = [((24, 20, 28), (1, 0, 0)), ((33, 17, 21), (0, 1, 1)), ((16, 16, 16), (1, 1, 1)),
+              ((40, 24, 16), (0, 0, 1)), ((20, 20, 20), (0, 0, 0)), ((18, 30, 12), (1, 1, 0))]
+    descs = [wave_desc(n3, 2, periodic=per, ko=0.1, precision=precision, dt=0.25 / n3[0], bc=TS_BC_DIRICHLET,
+                       bc_values=(0.25, -0.5)) for n3, per in shapes]
+    b = Batch(ctx, descs)
+    for i in range(len(descs)):
+        b.initialise(i, TS_INIT_GAUSSIAN, pulse(i))
+    b.step(4)
+    ctx.sync()
+    for i, d in enumerate(descs):
+        it = Integrator(ctx, d)
+        it.initialise(TS_INIT_GAUSSIAN, pulse(i))
+        it.step(4)
+        want = it.get_state()
+        got = b.get_state(i)
+        assert np.array_equal(got, want), (i, shapes[i], relerr(got, want))
+    b.close()
+
+
 def test_batch_fp64_matches_oracle(ctx, port_oracle):
     descs = batch_descs([20, (28, 16, 24)], 2, TS_F64, periodic=True, ko=0.1)
     b = Batch(ctx, descs)
