@@ -7,7 +7,7 @@
 // launch) and one producer warp. Per z plane:
 //
 //   * the producer warp's elected lane copies the plane's tile plus its ghost halo, all
-//     components, with one TMA load (cp.async.bulk.tensor.4d, no multicast; box
+//     components, with one TMA load (cp.async.bulk.tensor.4d into this CTA only; box
 //     (TX+2*XH) x (TY*CY+2G) x 1 x NC, zero fill outside the array) into a ring of R shared-memory
 //     slots. When the plane is also a stencil centre plane of this CTA, the same slot receives
 //     the epilogue's centre operands (the stage registers it reads at the centre cells, e.g.
